@@ -1,0 +1,341 @@
+"""Benchmark of the B200-native bld_mult solver.
+
+Default workload: a single large plain solve, x=1024, y=1024, z=64 (67M-element
+S, 512 MiB in FP64), 100 psi_appr iterations per step, FP64 storage.  A step is
+one 100-iteration solve; steps continue from the previous step's S, so every
+step does the same work.  S is larger than L2, so no L2 flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--dtype f64|f32]
+
+--impl reference times the reference algorithm's CPU path on this machine's
+host cores: the reference itself cannot be compiled here (it needs Eigen3 and
+GSL), so its OpenMP restatement in oracle/ stands in for it.
+
+With N > 1 (torchrun, one process per GPU) each rank solves its own replica:
+the solver does not shard (replicas only); value = all ranks' updates / the
+slowest rank's time.
+"""
+
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "bnmf-algs_b200")
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def load_package():
+    if "bnmf_algs_b200" in sys.modules:
+        return sys.modules["bnmf_algs_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "bnmf_algs_b200", os.path.join(PKG_DIR, "__init__.py"),
+        submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["bnmf_algs_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch of the sweep from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        rows = []
+        for l in self.lines:
+            p = [s.strip() for s in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), p[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_baseline_oracle(prob, target_s=10.0, threads=0):
+    """The oracle (reference restatement, OpenMP) on a bounded sample: whole
+    iterations of the same workload, as many as fit in about target_s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = O.set_threads(threads)
+    X, z = prob["X"], prob["z"]
+    S0 = O.init_S(X, z, 0)
+    t0 = time.perf_counter()
+    O.bld_mult(X, z, prob["alpha"], prob["beta"], 1, O.PSI_APPR, 1e-50, S0=S0)
+    one = time.perf_counter() - t0
+    n = max(1, min(int(target_s / max(one, 1e-6)), 50))
+    t0 = time.perf_counter()
+    O.bld_mult(X, z, prob["alpha"], prob["beta"], n, O.PSI_APPR, 1e-50, S0=S0)
+    dt = time.perf_counter() - t0
+    upd = X.size * z * n
+    return {"value": upd / dt, "unit": "S-updates/s", "cores": cores, "kind": "port",
+            "sample": f"{n} iterations of the full {X.shape[0]}x{X.shape[1]}x{z} workload "
+                      f"({dt:.1f} s, FP64, psi_appr, OpenMP {cores} threads)"}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    load_package()
+    import bnmf_algs_b200.workloads as W
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    prob = W.plain_large(1)
+    X, z = prob["X"], prob["z"]
+    cores = O.set_threads(0)
+    S = O.init_S(X, z, 0)
+    per_step = 1  # iterations of the full workload per step (bounded sample)
+    for _ in range(args.warmup):
+        S = O.bld_mult(X, z, prob["alpha"], prob["beta"], per_step, O.PSI_APPR, 1e-50, S0=S)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        S = O.bld_mult(X, z, prob["alpha"], prob["beta"], per_step, O.PSI_APPR, 1e-50, S0=S)
+    dt = time.perf_counter() - t0
+    value = X.size * z * per_step * args.steps / dt
+    line = {"impl": "reference", "metric": "S_elem_updates_per_s", "value": value,
+            "unit": "S-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "plain_1024x1024x64", "x": 1024, "y": 1024, "z": 64,
+                       "iters_per_step": per_step, "psi": "psi_appr", "storage": "f64",
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": "S-updates/s", "cores": cores,
+                             "kind": "port",
+                             "sample": f"{per_step} iteration(s) of the full 1024x1024x64 "
+                                       "workload per step; the reference is not buildable here "
+                                       "(Eigen3/GSL absent), its OpenMP restatement runs"},
+            "e2e": {"value": value, "unit": "S-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    pkg = load_package()
+    import bnmf_algs_b200.workloads as W
+    prob = W.plain_large(1)
+    X, z, iters = prob["X"], prob["z"], prob["iters"]
+    x, y = X.shape
+    f64 = args.dtype == "f64"
+    dt_t = torch.float64 if f64 else torch.float32
+    dtype = pkg.F64 if f64 else pkg.F32
+    es = 8 if f64 else 4
+    dev = torch.device("cuda", local)
+    dX = torch.as_tensor(X).to(dev, dt_t)
+    dalpha = torch.as_tensor(prob["alpha"]).to(dev)
+    dbeta = torch.as_tensor(prob["beta"]).to(dev)
+    dS = torch.empty((x, y, z), dtype=dt_t, device=dev)
+    plan = pkg.Plan(x, y, z, dtype)
+    plan.init_S(dX, dS, seed=0)
+    mode = pkg.PSI_APPR
+    stream = torch.cuda.current_stream()
+
+    def step():
+        plan.run(dX, dalpha, dbeta, dS, iters, mode, 1e-50, stream)
+
+    for _ in range(args.warmup):
+        step()
+    plan.check(stream)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = plan.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = plan.launch_count() - launches0
+    plan.check(stream)
+    ms = e0.elapsed_time(e1) / args.steps
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if dist:
+        dist.barrier()
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    upd_step = x * y * z * iters
+    value = upd_step * world / (ms_max / 1e3)
+
+    # Roofline of the fused update sweep: CUDA events around each launch.
+    kern_ms, iter_ms = plan.profile(dX, dalpha, dbeta, dS, 20, mode, 1e-50, stream)
+    alg_bytes = 2 * x * y * z * es + x * y * es
+    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+    peak, peak_src = hbm_peak()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src,
+                "traffic": profile_traffic(f"sweep_update_plain_1024x1024x64_{args.dtype}.md"),
+                "kernel": "sweep_kernel<UPDATE>", "kernel_ms": kern_ms,
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "iteration_ms": iter_ms,
+                "iteration_frac": alg_bytes / (iter_ms / 1e3) / 1e9 / peak}
+
+    # End to end through the public host-buffer C ABI (pinned host buffers,
+    # H2D of X and S0 and D2H of S inside every step).
+    hX = torch.as_tensor(X.astype(np.float64 if f64 else np.float32)).pin_memory()
+    hS0 = dS.cpu().pin_memory()
+    hS = torch.empty_like(hS0).pin_memory()
+    params = pkg.Params(prob["a"], prob["b"], prob["alpha"], prob["beta"])
+    cp = params.c_struct()
+    L = pkg.lib()
+    solve = L.bldm_solve_f64 if f64 else L.bldm_solve_f32
+    ptr_t = ctypes.POINTER(ctypes.c_double if f64 else ctypes.c_float)
+
+    def e2e_step():
+        rc = solve(ctypes.cast(hX.data_ptr(), ptr_t), x, y, z, ctypes.byref(cp), iters, mode,
+                   1e-50, ctypes.cast(hS0.data_ptr(), ptr_t), 0, ctypes.cast(hS.data_ptr(), ptr_t),
+                   None)
+        if rc != 0:
+            raise RuntimeError(f"bldm_solve failed with status {rc}")
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = upd_step * world / float(e2e_t.item())
+    h2d = x * y * es + x * y * z * es + (x + z) * 8
+    d2h = x * y * z * es
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_oracle(prob, target_s=args.cpu_seconds)
+
+    if rank == 0:
+        line = {"metric": "S_elem_updates_per_s", "value": value, "unit": "S-updates/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+                "config": {"workload": "plain_1024x1024x64", "x": x, "y": y, "z": z,
+                           "iters_per_step": iters, "psi": "psi_appr", "storage": args.dtype,
+                           "X_zero_fraction": float(np.mean(X == 0)),
+                           "l2": "inputs larger than L2 (S is 512 MiB in f64)",
+                           "parallelism": "replicas" if world > 1 else "single GPU"},
+                "hbm_gbs_iteration": alg_bytes / (ms_max / 1e3 / iters) / 1e9,
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": "S-updates/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
+                "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line))
+    plan.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--dtype", choices=["f64", "f32"], default="f64")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

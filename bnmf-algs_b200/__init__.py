@@ -1,0 +1,360 @@
+"""Python binding of libbldm.so, the B200-native bld_mult solver.
+
+Mirrors the reference interface of eozd/bnmf-algs for this path:
+
+* ``Params``          — alloc_model::Params (src/alloc_model/alloc_model_params.hpp:25-84)
+* ``bld_mult_cuda``   — bld::bld_mult_cuda (src/bld/bld_mult/bld_mult.hpp:225-324)
+* ``bld_mult``        — bld::bld_mult semantics (bld_mult.hpp:82-150), run on the GPU
+* ``log_marginal_S``  — alloc_model::log_marginal_S (src/alloc_model/alloc_model_funcs.hpp:573-586)
+
+Argument errors raise ``InvalidArgument`` (a ``ValueError``), the counterpart of
+the reference's ``BNMF_ASSERT`` throwing ``std::invalid_argument`` in test builds
+(src/defs.hpp:12-20).  Every call goes through the C ABI declared in
+include/bldm.h; there is no CPU fallback: if libbldm.so is missing or no GPU is
+present, the calls raise.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbldm.so")
+
+# bldm_status
+OK, ERR_BAD_ARG, ERR_NEG_X, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_NO_DEVICE, \
+    ERR_UNSUPPORTED, ERR_BUSY, ERR_NOT_FOUND = range(10)
+STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "NEG_X", 3: "OOM", 4: "CUDA", 5: "TIMEOUT",
+                6: "NO_DEVICE", 7: "UNSUPPORTED", 8: "BUSY", 9: "NOT_FOUND"}
+# bldm_psi_mode
+PSI_EXACT, PSI_APPR, PSI_LEGACY_CUDA = 0, 1, 2
+# bldm_dtype
+F64, F32 = 0, 1
+
+
+class BldmError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"bldm: {STATUS_NAMES.get(status, status)} {what}".strip())
+
+
+class InvalidArgument(ValueError):
+    """Raised where the reference's BNMF_ASSERT throws std::invalid_argument."""
+
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"bldm: {STATUS_NAMES.get(status, status)} {what}".strip())
+
+
+def _check(rc, what=""):
+    if rc == OK:
+        return
+    if rc in (ERR_BAD_ARG, ERR_NEG_X):
+        raise InvalidArgument(rc, what)
+    raise BldmError(rc, what)
+
+
+class bldm_params(ctypes.Structure):
+    _fields_ = [("a", ctypes.c_double), ("b", ctypes.c_double),
+                ("alpha", ctypes.POINTER(ctypes.c_double)), ("n_alpha", ctypes.c_size_t),
+                ("beta", ctypes.POINTER(ctypes.c_double)), ("n_beta", ctypes.c_size_t)]
+
+
+class bldm_stats(ctypes.Structure):
+    _fields_ = [("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("iterations", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
+                ("rel_change", ctypes.c_double)]
+
+
+_lib = None
+_vp = ctypes.c_void_p
+_sz = ctypes.c_size_t
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def lib():
+    """The loaded libbldm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise BldmError(ERR_NO_DEVICE, f"{LIB_PATH} is missing; run build()")
+        L = ctypes.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def build(force=False):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_bldm_build", os.path.join(_HERE, "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.build(force=force)
+
+
+# Every symbol include/bldm.h declares, with (restype, argtypes).
+SIGNATURES = {
+    "bldm_solve_f64": (ctypes.c_int, [_dp, _sz, _sz, _sz, ctypes.POINTER(bldm_params), _sz,
+                                      ctypes.c_int, ctypes.c_double, _dp, ctypes.c_uint64, _dp,
+                                      ctypes.POINTER(bldm_stats)]),
+    "bldm_solve_f32": (ctypes.c_int, [_fp, _sz, _sz, _sz, ctypes.POINTER(bldm_params), _sz,
+                                      ctypes.c_int, ctypes.c_double, _fp, ctypes.c_uint64, _fp,
+                                      ctypes.POINTER(bldm_stats)]),
+    "bldm_release_cache": (ctypes.c_int, []),
+    "bldm_plan_create": (ctypes.c_int, [ctypes.POINTER(_vp), _sz, _sz, _sz, ctypes.c_int]),
+    "bldm_plan_destroy": (ctypes.c_int, [_vp]),
+    "bldm_plan_workspace_bytes": (ctypes.c_int, [_vp, ctypes.POINTER(_sz)]),
+    "bldm_plan_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _sz, ctypes.c_int, ctypes.c_double,
+                                     _vp]),
+    "bldm_plan_check": (ctypes.c_int, [_vp, _vp]),
+    "bldm_plan_init_S": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp]),
+    "bldm_plan_profile": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _sz, ctypes.c_int,
+                                         ctypes.c_double, _vp, _dp, _dp]),
+    "bldm_plan_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "bldm_tensor_sums_f64": (ctypes.c_int, [_vp, _sz, _sz, _sz, _vp, _vp, _vp, _vp]),
+    "bldm_update_grad_plus_f64": (ctypes.c_int, [_vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp,
+                                                 _vp]),
+    "bldm_update_grad_minus_f64": (ctypes.c_int, [_vp, _sz, _sz, ctypes.c_int, _vp, _vp]),
+    "bldm_update_nom_f64": (ctypes.c_int, [_vp, _vp, _vp, _sz, _sz, _sz, _vp, _vp]),
+    "bldm_update_denom_f64": (ctypes.c_int, [_vp, _vp, _vp, _sz, _sz, _sz, _vp, _vp]),
+    "bldm_update_S_f64": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz,
+                                         ctypes.c_double, _vp, _vp]),
+    "bldm_psi_f64": (ctypes.c_int, [_vp, _sz, ctypes.c_int, _vp, _vp]),
+    "bldm_psi_f32": (ctypes.c_int, [_vp, _sz, _vp, _vp]),
+    "bldm_log_marginal_S": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _sz, _sz, _dp, _dp,
+                                           ctypes.c_double, ctypes.c_double, _dp, _vp]),
+    "bldm_version": (ctypes.c_char_p, []),
+}
+
+
+def _declare(L):
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def version():
+    return lib().bldm_version().decode()
+
+
+class Params:
+    """alloc_model::Params: Gamma shape a, rate b, Dirichlet alpha (x) and beta (z)."""
+
+    def __init__(self, a, b, alpha, beta):
+        self.a = float(a)
+        self.b = float(b)
+        self.alpha = np.ascontiguousarray(alpha, dtype=np.float64).reshape(-1)
+        self.beta = np.ascontiguousarray(beta, dtype=np.float64).reshape(-1)
+
+    @classmethod
+    def from_shape(cls, shape):
+        """The reference's default ctor from a tensor shape: a=1, b=10, alpha=1, beta=1."""
+        x, _, z = shape
+        return cls(1.0, 10.0, np.ones(x), np.ones(z))
+
+    def c_struct(self):
+        p = bldm_params()
+        p.a, p.b = self.a, self.b
+        p.alpha = self.alpha.ctypes.data_as(_dp)
+        p.n_alpha = self.alpha.size
+        p.beta = self.beta.ctypes.data_as(_dp)
+        p.n_beta = self.beta.size
+        return p
+
+
+def _solve(X, z, params, max_iter, psi_mode, eps, S0, seed, dtype, stats):
+    np_t = np.float64 if dtype == F64 else np.float32
+    X = np.ascontiguousarray(X, dtype=np_t)
+    if X.ndim != 2:
+        raise InvalidArgument(ERR_BAD_ARG, "X must be a matrix")
+    x, y = X.shape
+    out = np.empty((x, y, int(z)), dtype=np_t)
+    S0p = None
+    if S0 is not None:
+        S0 = np.ascontiguousarray(S0, dtype=np_t)
+        if S0.shape != out.shape:
+            raise InvalidArgument(ERR_BAD_ARG, "S0 shape")
+    cp = params.c_struct()
+    st = bldm_stats()
+    if dtype == F64:
+        ptr = lambda a: a.ctypes.data_as(_dp) if a is not None else None
+        rc = lib().bldm_solve_f64(ptr(X), x, y, int(z), ctypes.byref(cp), int(max_iter),
+                                  int(psi_mode), float(eps), ptr(S0), int(seed), ptr(out),
+                                  ctypes.byref(st))
+    else:
+        ptr = lambda a: a.ctypes.data_as(_fp) if a is not None else None
+        rc = lib().bldm_solve_f32(ptr(X), x, y, int(z), ctypes.byref(cp), int(max_iter),
+                                  int(psi_mode), float(eps), ptr(S0), int(seed), ptr(out),
+                                  ctypes.byref(st))
+    _check(rc, "bldm_solve")
+    if stats is not None:
+        stats.update(device_ms=st.device_ms, total_ms=st.total_ms, iterations=st.iterations,
+                     kernel_launches=st.kernel_launches)
+    return out
+
+
+def bld_mult_cuda(X, z, params, max_iter=1000, use_psi_appr=False, eps=1e-50, S0=None, seed=0,
+                  dtype=F64, stats=None):
+    """bld::bld_mult_cuda: with use_psi_appr=False the grad_plus digamma stays psi_appr,
+    as in the reference's device kernel; grad_minus uses the exact digamma."""
+    mode = PSI_APPR if use_psi_appr else PSI_LEGACY_CUDA
+    return _solve(X, z, params, max_iter, mode, eps, S0, seed, dtype, stats)
+
+
+def bld_mult(X, z, params, max_iter=1000, use_psi_appr=False, eps=1e-50, S0=None, seed=0,
+             dtype=F64, stats=None):
+    """bld::bld_mult semantics (exact digamma everywhere unless use_psi_appr), on the GPU."""
+    mode = PSI_APPR if use_psi_appr else PSI_EXACT
+    return _solve(X, z, params, max_iter, mode, eps, S0, seed, dtype, stats)
+
+
+def release_cache():
+    _check(lib().bldm_release_cache())
+
+
+# ----------------------------------------------------------------------------
+# Device-buffer API (torch CUDA tensors as the device allocator).
+# ----------------------------------------------------------------------------
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Plan:
+    """bldm_plan: workspace for one (x, y, z, dtype); runs on device tensors."""
+
+    def __init__(self, x, y, z, dtype=F64):
+        self._h = ctypes.c_void_p()
+        self.shape = (x, y, z)
+        self.dtype = dtype
+        _check(lib().bldm_plan_create(ctypes.byref(self._h), x, y, z, dtype), "plan_create")
+
+    def close(self):
+        if self._h:
+            lib().bldm_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def workspace_bytes(self):
+        n = ctypes.c_size_t()
+        _check(lib().bldm_plan_workspace_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
+    def run(self, dX, dalpha, dbeta, dS, max_iter, psi_mode=PSI_APPR, eps=1e-50, stream=None):
+        _check(lib().bldm_plan_run(self._h, _ptr(dX), _ptr(dalpha), _ptr(dbeta), _ptr(dS),
+                                   int(max_iter), int(psi_mode), float(eps),
+                                   _stream_ptr(stream)), "plan_run")
+
+    def check(self, stream=None):
+        _check(lib().bldm_plan_check(self._h, _stream_ptr(stream)), "plan_check")
+
+    def init_S(self, dX, dS, seed=0, stream=None):
+        _check(lib().bldm_plan_init_S(self._h, _ptr(dX), _ptr(dS), int(seed),
+                                      _stream_ptr(stream)))
+
+    def profile(self, dX, dalpha, dbeta, dS, iters, psi_mode=PSI_APPR, eps=1e-50, stream=None):
+        k = ctypes.c_double()
+        it = ctypes.c_double()
+        _check(lib().bldm_plan_profile(self._h, _ptr(dX), _ptr(dalpha), _ptr(dbeta), _ptr(dS),
+                                       int(iters), int(psi_mode), float(eps), _stream_ptr(stream),
+                                       ctypes.byref(k), ctypes.byref(it)), "plan_profile")
+        return k.value, it.value
+
+    def launch_count(self):
+        n = ctypes.c_uint64()
+        _check(lib().bldm_plan_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+
+def log_marginal_S(dS, params, dtype=F64, stream=None):
+    """alloc_model::log_marginal_S of a device tensor, on the device (FP64)."""
+    x, y, z = dS.shape
+    out = ctypes.c_double()
+    _check(lib().bldm_log_marginal_S(_ptr(dS), dtype, x, y, z,
+                                     params.alpha.ctypes.data_as(_dp),
+                                     params.beta.ctypes.data_as(_dp), params.a, params.b,
+                                     ctypes.byref(out), _stream_ptr(stream)), "log_marginal_S")
+    return out.value
+
+
+# Per-stage device functions (FP64 torch tensors), mirroring the reference's
+# update_*_cuda host functions.
+def tensor_sums(dS, stream=None):
+    import torch
+    x, y, z = dS.shape
+    pjk = torch.empty((y, z), dtype=torch.float64, device=dS.device)
+    ipk = torch.empty((x, z), dtype=torch.float64, device=dS.device)
+    ijp = torch.empty((x, y), dtype=torch.float64, device=dS.device)
+    _check(lib().bldm_tensor_sums_f64(_ptr(dS), x, y, z, _ptr(pjk), _ptr(ipk), _ptr(ijp),
+                                      _stream_ptr(stream)))
+    return pjk, ipk, ijp
+
+
+def update_grad_plus(dS, dbeta_eph, appr=True, stream=None):
+    import torch
+    x, y, z = dS.shape
+    out = torch.empty_like(dS)
+    _check(lib().bldm_update_grad_plus_f64(_ptr(dS), _ptr(dbeta_eph), x, y, z, int(appr),
+                                           _ptr(out), _stream_ptr(stream)))
+    return out
+
+
+def update_grad_minus(dalpha_eph, appr=True, stream=None):
+    import torch
+    x, z = dalpha_eph.shape
+    out = torch.empty_like(dalpha_eph)
+    _check(lib().bldm_update_grad_minus_f64(_ptr(dalpha_eph), x, z, int(appr), _ptr(out),
+                                            _stream_ptr(stream)))
+    return out
+
+
+def update_nom(dXr, dgm, dS, stream=None):
+    import torch
+    x, y, z = dS.shape
+    out = torch.empty((x, y), dtype=torch.float64, device=dS.device)
+    _check(lib().bldm_update_nom_f64(_ptr(dXr), _ptr(dgm), _ptr(dS), x, y, z, _ptr(out),
+                                     _stream_ptr(stream)))
+    return out
+
+
+def update_denom(dXr, dgp, dS, stream=None):
+    import torch
+    x, y, z = dS.shape
+    out = torch.empty((x, y), dtype=torch.float64, device=dS.device)
+    _check(lib().bldm_update_denom_f64(_ptr(dXr), _ptr(dgp), _ptr(dS), x, y, z, _ptr(out),
+                                       _stream_ptr(stream)))
+    return out
+
+
+def update_S(dX, dnom, ddenom, dgm, dgp, dijp, dS, eps=1e-50, stream=None):
+    """In place on dS."""
+    x, y, z = dS.shape
+    _check(lib().bldm_update_S_f64(_ptr(dX), _ptr(dnom), _ptr(ddenom), _ptr(dgm), _ptr(dgp),
+                                   _ptr(dijp), x, y, z, float(eps), _ptr(dS),
+                                   _stream_ptr(stream)))
+    return dS
+
+
+def psi(d_in, appr=True, stream=None):
+    import torch
+    out = torch.empty_like(d_in)
+    if d_in.dtype == torch.float64:
+        _check(lib().bldm_psi_f64(_ptr(d_in), d_in.numel(), int(appr), _ptr(out),
+                                  _stream_ptr(stream)))
+    else:
+        _check(lib().bldm_psi_f32(_ptr(d_in), d_in.numel(), _ptr(out), _stream_ptr(stream)))
+    return out

@@ -1,0 +1,237 @@
+// Device building blocks shared by the bld_mult kernels: digamma in FP64 and
+// FP32, warp reductions, and thin wrappers over the sm_100a bulk-copy (TMA
+// engine, non-tensor form) and mbarrier PTX used to stage S slabs in shared
+// memory.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bldm {
+
+enum PsiMode : int { PSI_EXACT = 0, PSI_APPR = 1, PSI_LEGACY_CUDA = 2 };
+
+// Error bits written into the device error word.
+enum DevErr : int { DEV_ERR_WAIT_TIMEOUT = 1, DEV_ERR_BAD_LAUNCH = 2 };
+
+// A bounded wait gives up after this many nanoseconds of %globaltimer.
+constexpr unsigned long long kWaitLimitNs = 1000000000ull;
+
+// ---------------------------------------------------------------------------
+// Digamma.
+//
+// psi_appr restates util::psi_appr (src/util/util.hpp:440-514): unit shifts by
+// psi(x) = psi(x + 1) - 1/x until the argument is >= 6 (x < 1 shifts by 6,
+// [n, n+1) by 6 - n), then the asymptotic series
+//   ln x - 1/(2x) - 1/(12x^2) + 1/(120x^4) - 1/(252x^6) + 1/(240x^8)
+//        - 1/(132x^10) + 691/(32760x^12) - 1/(12x^14).
+// The exact digamma (the reference calls gsl_sf_psi) is the same published
+// method (Abramowitz & Stegun 6.3.5 and 6.3.18) with threshold 10 and one more
+// term, 3617/(8160x^16); its truncation error is below 5e-17.
+//
+// Both are branch-free: the shift sum sum_m 1/(x+m) is accumulated as one
+// fraction N/D and a single division 1/(x' D) yields both 1/x' and N/D.
+// ---------------------------------------------------------------------------
+template <int THRESH, bool EXTRA_TERM>
+__device__ __forceinline__ double psi_f64(double x) {
+    double n = 0.0;
+    if (x < double(THRESH)) {
+        n = double(THRESH) - floor(x);
+        n = n > double(THRESH) ? double(THRESH) : n;  // x < 1 shifts by THRESH
+    }
+    double num = 0.0, den = 1.0;
+#pragma unroll
+    for (int m = 0; m < THRESH; ++m) {
+        const bool act = double(m) < n;
+        const double f = act ? x + double(m) : 1.0;
+        num = act ? fma(num, f, den) : num;
+        den = den * f;
+    }
+    const double xs = x + n;
+    const double inv = 1.0 / (xs * den);
+    const double r = den * inv;       // 1 / xs
+    const double shift = num * xs * inv;  // sum_m 1/(x+m)
+    const double r2 = r * r;
+    double t;
+    if (EXTRA_TERM) {
+        t = fma(r2, -3617.0 / 8160.0, 1.0 / 12.0);
+        t = fma(r2, -t, 691.0 / 32760.0);
+    } else {
+        t = fma(r2, -1.0 / 12.0, 691.0 / 32760.0);
+    }
+    t = fma(r2, -t, 1.0 / 132.0);
+    t = fma(r2, -t, 1.0 / 240.0);
+    t = fma(r2, -t, 1.0 / 252.0);
+    t = fma(r2, -t, 1.0 / 120.0);
+    t = fma(r2, -t, 1.0 / 12.0);
+    return log(xs) - 0.5 * r - r2 * t - shift;
+}
+
+__device__ __forceinline__ double psi_appr_f64(double x) { return psi_f64<6, false>(x); }
+__device__ __forceinline__ double psi_exact_f64(double x) {
+    return x > 0.0 ? psi_f64<10, true>(x) : __longlong_as_double(0x7ff8000000000000ll);
+}
+
+// FP32 digamma for FP32 storage: the same shift rule (threshold 6) and the
+// series truncated after the x^-8 term, whose omitted remainder at x >= 6 is
+// below 2e-10, far under FP32 resolution.  Written in 1/x so that it does not
+// overflow for large counts.
+__device__ __forceinline__ float psi_f32(float x) {
+    float n = 0.f;
+    if (x < 6.f) {
+        n = 6.f - floorf(x);
+        n = n > 6.f ? 6.f : n;
+    }
+    float num = 0.f, den = 1.f;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const bool act = float(m) < n;
+        const float f = act ? x + float(m) : 1.f;
+        num = act ? fmaf(num, f, den) : num;
+        den = den * f;
+    }
+    const float xs = x + n;
+    const float inv = 1.f / (xs * den);
+    const float r = den * inv;
+    const float shift = num * xs * inv;
+    const float r2 = r * r;
+    float t = fmaf(r2, -1.f / 240.f, 1.f / 252.f);
+    t = fmaf(r2, -t, 1.f / 120.f);
+    t = fmaf(r2, -t, 1.f / 12.f);
+    return logf(xs) - 0.5f * r - r2 * t - shift;
+}
+
+template <typename T> struct Psi;
+template <> struct Psi<double> {
+    __device__ __forceinline__ static double appr(double v) { return psi_appr_f64(v); }
+    __device__ __forceinline__ static double exact(double v) { return psi_exact_f64(v); }
+};
+template <> struct Psi<float> {
+    __device__ __forceinline__ static float appr(float v) { return psi_f32(v); }
+    __device__ __forceinline__ static float exact(float v) { return psi_f32(v); }
+};
+
+__device__ __forceinline__ double psi_mode_f64(double v, bool appr) {
+    return appr ? psi_appr_f64(v) : psi_exact_f64(v);
+}
+
+// ---------------------------------------------------------------------------
+// Timers, bounded waits, bulk copies.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for the phase with the given parity to complete; false after
+// kWaitLimitNs without completion.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > kWaitLimitNs) return false;
+    }
+}
+
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// Global -> shared bulk copy (no tensor map, no multicast), completing on the
+// mbarrier's transaction count.  dst/src 16-byte aligned, bytes % 16 == 0.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar, uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+        : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Warp reductions over aligned lane groups of width W (power of two).
+// ---------------------------------------------------------------------------
+template <int W, typename V> __device__ __forceinline__ V group_sum(V v) {
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum across lanes that share (lane % LPF): offsets LPF, 2 LPF, ..., 16.
+template <int LPF, typename V> __device__ __forceinline__ V cross_group_sum(V v) {
+#pragma unroll
+    for (int o = LPF; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Kahan-compensated FP32 accumulator (sum s, running compensation c).
+struct KahanF {
+    float s, c;
+    __device__ __forceinline__ void init() { s = 0.f; c = 0.f; }
+    __device__ __forceinline__ void add(float v) {
+        const float yv = v - c;
+        const float t = s + yv;
+        c = (t - s) - yv;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return double(s) - double(c); }
+};
+
+// Accumulator selection: FP64 storage accumulates in double, FP32 storage in
+// Kahan-compensated float pairs.
+template <typename T> struct Acc;
+template <> struct Acc<double> {
+    double s;
+    __device__ __forceinline__ void init() { s = 0.0; }
+    __device__ __forceinline__ void add(double v) { s += v; }
+    __device__ __forceinline__ double value() const { return s; }
+};
+template <> struct Acc<float> {
+    KahanF k;
+    __device__ __forceinline__ void init() { k.init(); }
+    __device__ __forceinline__ void add(float v) { k.add(v); }
+    __device__ __forceinline__ double value() const { return k.value(); }
+};
+
+}  // namespace bldm

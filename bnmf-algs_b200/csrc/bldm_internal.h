@@ -1,0 +1,69 @@
+// Host-side internals shared by the translation units of libbldm.so.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/bldm.h"
+
+namespace bldm {
+
+// Launch configuration of the fused sweep for one shape.
+//
+// The (i, j) plane of S is cut into CTA regions: a band of `band_w`
+// consecutive columns j (contiguous fibers of one row, so one bulk copy per
+// row) times a range of rows.  Region (band, rr) writes one row of S_pjk
+// partials [rr][j in band][k] and, per row, one row of S_ipk partials
+// [band][i][k]; the finalize kernel sums them in a fixed order.
+struct SweepCfg {
+    int vec;        // elements per lane access (16 / sizeof(T) when aligned)
+    int lpf;        // lanes per fiber
+    int mch;        // chunks (of vec elements) per lane
+    int cpw;        // fiber passes per warp per row
+    int warps;      // warps per CTA
+    int band_w;     // columns per band
+    int n_bands;
+    int n_rr;       // row ranges
+    int rr_base, rr_extra;
+    int stages;     // bulk-copy pipeline depth
+    int ctas_per_sm;  // resident sweep CTAs per SM (shared-memory bound)
+    uint32_t capS, capX, capA;  // bytes per stage of each slab
+    uint32_t stage_bytes;
+    size_t smem_update, smem_sums;
+    int n_ablk, rows_per_ablk;  // finalize: row blocks for alpha_eph
+    int fin_threads;
+};
+
+struct PlanImpl {
+    int device = 0;
+    int dtype = BLDM_F64;
+    size_t x = 0, y = 0, z = 0;
+    size_t esize = 8;
+    SweepCfg cfg{};
+    // Workspace: one allocation carved into the pieces below.
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    double* part_pjk = nullptr;   // [n_rr][y][z]
+    double* part_ipk = nullptr;   // [n_bands][x][z]
+    void* psiB = nullptr;         // [y][z]  T
+    void* psiA = nullptr;         // [x][z]  T
+    void* psiAS = nullptr;        // [z]     T
+    double* asum_part = nullptr;  // [n_ablk][z]
+    unsigned* counter = nullptr;  // finalize last-block counter
+    int* err = nullptr;           // device error word
+    uint64_t launches = 0;
+};
+
+// Implemented in bldm_sweep.cu.
+int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype);
+void plan_free(PlanImpl* p);
+int plan_run(PlanImpl* p, const void* dX, const double* dalpha, const double* dbeta,
+             void* dS, size_t max_iter, int psi_mode, double eps, cudaStream_t st,
+             cudaEvent_t* kernel_events, size_t n_kernel_events);
+int plan_init_S(PlanImpl* p, const void* dX, void* dS, uint64_t seed, cudaStream_t st);
+int plan_check(PlanImpl* p, cudaStream_t st);
+
+int cuda_status(cudaError_t e);
+
+}  // namespace bldm

@@ -1,0 +1,211 @@
+/*
+ * bldm.h — C ABI of the B200-native multiplicative-update Best Latent
+ * Decomposition solver (libbldm.so).
+ *
+ * The reference (eozd/bnmf-algs) exposes this path as C++ templates only:
+ *
+ *   template <typename T, typename Scalar>
+ *   tensor_t<T, 3> bld::bld_mult(const matrix_t<T>& X, size_t z,
+ *                               const alloc_model::Params<Scalar>& params,
+ *                               size_t max_iter = 1000,
+ *                               bool use_psi_appr = false,
+ *                               double eps = 1e-50);
+ *   (src/bld/bld_mult/bld_mult.hpp:82-86; bld_mult_cuda at :225-229 has the
+ *   same signature)
+ *
+ * These entry points are what that template binds to (see the header-only
+ * C++14 mirror bnmf-algs_b200/cpp/bnmf_algs_b200/bld_mult.hpp).  Plain
+ * pointers and sizes only.  Layouts are row-major like the reference's
+ * matrix_t / tensor_t (src/defs.hpp:40-52): X(i,j) at i*y+j and S(i,j,k) at
+ * (i*y+j)*z+k.  Every function returns a bldm_status.
+ */
+#ifndef BLDM_H_
+#define BLDM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference reports argument errors with BNMF_ASSERT
+ * (src/defs.hpp:12-20), which throws std::invalid_argument in test builds;
+ * the C++ mirror maps BLDM_ERR_BAD_ARG and BLDM_ERR_NEG_X to that exception
+ * and every other failure to std::runtime_error. */
+typedef enum bldm_status {
+    BLDM_OK = 0,
+    BLDM_ERR_BAD_ARG = 1,     /* null pointer, size mismatch (alpha != x, beta != z) */
+    BLDM_ERR_NEG_X = 2,       /* X has a negative or NaN entry (check_bld_params) */
+    BLDM_ERR_OOM = 3,         /* device allocation failed */
+    BLDM_ERR_CUDA = 4,        /* a CUDA runtime call or launch failed */
+    BLDM_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+    BLDM_ERR_NO_DEVICE = 6,   /* no usable CUDA device */
+    BLDM_ERR_UNSUPPORTED = 7, /* shape outside the fused kernels' range (z too large) */
+    BLDM_ERR_BUSY = 8,        /* serving: no slot or memory for the request now */
+    BLDM_ERR_NOT_FOUND = 9    /* serving: unknown request id */
+} bldm_status;
+
+/* Digamma selection.
+ *   BLDM_PSI_EXACT       — exact digamma everywhere: bld::bld_mult with
+ *                          use_psi_appr=false (bld_mult.hpp:119-120).
+ *   BLDM_PSI_APPR        — util::psi_appr everywhere (use_psi_appr=true).
+ *   BLDM_PSI_LEGACY_CUDA — bld::bld_mult_cuda with use_psi_appr=false: its
+ *                          grad_plus kernel always uses psi_appr
+ *                          (cuda_src/bld_mult/bld_mult_cuda_kernels.cu:116)
+ *                          while grad_minus uses the exact digamma
+ *                          (bld_mult.hpp:286,309). */
+typedef enum bldm_psi_mode {
+    BLDM_PSI_EXACT = 0,
+    BLDM_PSI_APPR = 1,
+    BLDM_PSI_LEGACY_CUDA = 2
+} bldm_psi_mode;
+
+/* Storage precision of S and X on the device. */
+typedef enum bldm_dtype { BLDM_F64 = 0, BLDM_F32 = 1 } bldm_dtype;
+
+/* alloc_model::Params<Scalar> (src/alloc_model/alloc_model_params.hpp:25-84):
+ * Gamma shape a and rate b, Dirichlet parameters alpha (length x) and beta
+ * (length z).  a and b are not used by bld_mult itself; they are carried for
+ * log_marginal_S. */
+typedef struct bldm_params {
+    double a;
+    double b;
+    const double* alpha;
+    size_t n_alpha;
+    const double* beta;
+    size_t n_beta;
+} bldm_params;
+
+/* Per-call statistics (optional output; pass NULL to skip). */
+typedef struct bldm_stats {
+    double device_ms;       /* device time of the iterations (CUDA events) */
+    double total_ms;        /* host wall time of the whole call */
+    uint64_t iterations;    /* iterations run */
+    uint64_t kernel_launches; /* kernels launched by the call */
+    double rel_change;      /* ||S_last - S_prev||_1 / ||S_last||_1 (batch/server) */
+} bldm_stats;
+
+/* ------------------------------------------------------------------------
+ * Drop-in host-buffer solve.
+ *
+ * Replaces bld::bld_mult_cuda (src/bld/bld_mult/bld_mult.hpp:225-324) and,
+ * with BLDM_PSI_EXACT, bld::bld_mult (bld_mult.hpp:82-150).  X (x*y) and the
+ * result S_out (x*y*z) are HOST buffers (pinned memory makes the copies
+ * faster but is not required).  S0 (x*y*z, host) is the initial allocation
+ * tensor; when NULL it is drawn on the device as S(i,j,:) = X(i,j) *
+ * Dirichlet(1_z) from a counter-based generator seeded with `seed` (the
+ * reference's init_S, bld_mult_funcs.hpp:36-74, is GSL-seeded and
+ * thread-count dependent).  The call is synchronous.  Device buffers are
+ * kept in a per-device cache between calls of the same shape (release them
+ * with bldm_release_cache).
+ *
+ * _f64: FP64 storage and arithmetic.  _f32: FP32 storage and arithmetic with
+ * Kahan-compensated axis sums; X and S are FP32 host buffers.
+ * ---------------------------------------------------------------------- */
+int bldm_solve_f64(const double* X, size_t x, size_t y, size_t z,
+                   const bldm_params* params, size_t max_iter, int psi_mode,
+                   double eps, const double* S0, uint64_t seed, double* S_out,
+                   bldm_stats* stats);
+int bldm_solve_f32(const float* X, size_t x, size_t y, size_t z,
+                   const bldm_params* params, size_t max_iter, int psi_mode,
+                   double eps, const float* S0, uint64_t seed, float* S_out,
+                   bldm_stats* stats);
+
+/* Free the device buffers cached by bldm_solve_* on the current device. */
+int bldm_release_cache(void);
+
+/* ------------------------------------------------------------------------
+ * Device-buffer plan.  For callers that keep X and S resident in HBM
+ * (serving, frameworks).  A plan owns the solver's workspace for one shape.
+ * d_X (x*y), d_S (x*y*z) are device buffers of the plan's dtype, 16-byte
+ * aligned and allocated in multiples of 16 bytes (cudaMalloc and the torch
+ * caching allocator both satisfy this); d_alpha (x) and d_beta (z) are FP64
+ * device buffers.  d_S holds S0 on entry and the solution on return.  Work
+ * is enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) and
+ * the call returns without synchronising; bldm_plan_check asynchronously
+ * surfaces a device-side error once the stream has drained.
+ * ---------------------------------------------------------------------- */
+typedef struct bldm_plan bldm_plan;
+
+int bldm_plan_create(bldm_plan** plan, size_t x, size_t y, size_t z, int dtype);
+int bldm_plan_destroy(bldm_plan* plan);
+/* Bytes of device workspace the plan holds (partials, digamma tables). */
+int bldm_plan_workspace_bytes(const bldm_plan* plan, size_t* bytes);
+int bldm_plan_run(bldm_plan* plan, const void* d_X, const double* d_alpha,
+                  const double* d_beta, void* d_S, size_t max_iter,
+                  int psi_mode, double eps, void* stream);
+/* Synchronises `stream` and reports a device-side error recorded by the
+ * plan's kernels (BLDM_ERR_TIMEOUT) or a CUDA error. */
+int bldm_plan_check(bldm_plan* plan, void* stream);
+/* Draw the seeded initial S on the device (see bldm_solve_f64). */
+int bldm_plan_init_S(bldm_plan* plan, const void* d_X, void* d_S, uint64_t seed,
+                     void* stream);
+/* Run `iters` iterations with CUDA events around every launch of the fused
+ * update kernel and report its mean duration (ms) and the mean duration of
+ * one whole iteration (ms).  Used to place the kernel on the HBM roofline. */
+int bldm_plan_profile(bldm_plan* plan, const void* d_X, const double* d_alpha,
+                      const double* d_beta, void* d_S, size_t iters,
+                      int psi_mode, double eps, void* stream,
+                      double* update_kernel_ms, double* iteration_ms);
+/* Kernels launched by the plan since creation. */
+int bldm_plan_launch_count(const bldm_plan* plan, uint64_t* count);
+
+/* ------------------------------------------------------------------------
+ * Per-stage device functions.  Each mirrors one function of the reference's
+ * CUDA host side so that every formula can be checked against the CPU
+ * restatement on its own (the reference's test strategy,
+ * test/bld/bld_mult/test_bld_mult_cuda_funcs.cpp).  All pointers are FP64
+ * device buffers, row-major, unpadded; work goes to `stream`.
+ * ---------------------------------------------------------------------- */
+/* cuda::tensor_sums (cuda_src/tensor_ops.cu:10-55): S_pjk (y*z), S_ipk
+ * (x*z), S_ijp (x*y). */
+int bldm_tensor_sums_f64(const double* d_S, size_t x, size_t y, size_t z,
+                         double* d_pjk, double* d_ipk, double* d_ijp,
+                         void* stream);
+/* update_grad_plus_cuda (cuda_src/bld_mult/bld_mult_cuda_funcs.cu:8-33):
+ * gp(i,j,k) = psi(beta_eph(j,k)) - psi(S(i,j,k)+1).  appr != 0 selects
+ * psi_appr (the reference kernel always does). */
+int bldm_update_grad_plus_f64(const double* d_S, const double* d_beta_eph,
+                              size_t x, size_t y, size_t z, int appr,
+                              double* d_grad_plus, void* stream);
+/* update_grad_minus (bld_mult_funcs.hpp:205-229; host-side in the
+ * reference): gm(i,k) = psi(sum_i alpha_eph(i,k)) - psi(alpha_eph(i,k)). */
+int bldm_update_grad_minus_f64(const double* d_alpha_eph, size_t x, size_t z,
+                               int appr, double* d_grad_minus, void* stream);
+/* update_nom_cuda (bld_mult_cuda_funcs.cu:36-61):
+ * nom(i,j) = sum_k S(i,j,k) Xr(i,j) gm(i,k). */
+int bldm_update_nom_f64(const double* d_X_reciprocal, const double* d_grad_minus,
+                        const double* d_S, size_t x, size_t y, size_t z,
+                        double* d_nom, void* stream);
+/* update_denom_cuda (bld_mult_cuda_funcs.cu:64-88):
+ * denom(i,j) = sum_k S(i,j,k) Xr(i,j) gp(i,j,k). */
+int bldm_update_denom_f64(const double* d_X_reciprocal, const double* d_grad_plus,
+                          const double* d_S, size_t x, size_t y, size_t z,
+                          double* d_denom, void* stream);
+/* update_S_cuda (bld_mult_cuda_funcs.cu:91-120), with the caller's eps (the
+ * reference kernel hard-codes 1e-50, bld_mult_cuda_kernels.cu:209). */
+int bldm_update_S_f64(const double* d_X, const double* d_nom,
+                      const double* d_denom, const double* d_grad_minus,
+                      const double* d_grad_plus, const double* d_S_ijp,
+                      size_t x, size_t y, size_t z, double eps, double* d_S,
+                      void* stream);
+/* util::psi_appr / exact digamma over an array (appr != 0: psi_appr). */
+int bldm_psi_f64(const double* d_in, size_t n, int appr, double* d_out, void* stream);
+int bldm_psi_f32(const float* d_in, size_t n, float* d_out, void* stream);
+
+/* alloc_model::log_marginal_S (src/alloc_model/alloc_model_funcs.hpp:573-586)
+ * of a device tensor, computed on the device in FP64.  d_S is FP64 or FP32
+ * per dtype; alpha (x) and beta (z) are HOST arrays. */
+int bldm_log_marginal_S(const void* d_S, int dtype, size_t x, size_t y, size_t z,
+                        const double* alpha, const double* beta, double a,
+                        double b, double* result, void* stream);
+
+/* Library version string. */
+const char* bldm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BLDM_H_ */

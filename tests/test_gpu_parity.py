@@ -1,0 +1,292 @@
+"""GPU parity of libbldm.so against the CPU oracle.
+
+Tolerances (FP64 storage): per-stage results within Eigen's default isApprox
+precision for double (1e-12), as the reference's
+test/bld/bld_mult/test_bld_mult_cuda_funcs.cpp requires; whole solves within
+1e-9 relative (max-norm relative error), the bar the reference's FP64 build
+is held to.  FP32 storage is compared with the FP64 oracle at the tolerance
+stated in each test.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def rel_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = max(np.abs(b).max(), 1e-300)
+    return float(np.abs(a - b).max() / scale)
+
+
+def dev(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+# ---------------------------------------------------------------- digamma
+def test_psi_appr_and_exact_match_oracle(bldm, oracle, psi_points):
+    rng = np.random.default_rng(0)
+    pts = np.concatenate([psi_points["points"], rng.uniform(1e-6, 1, 5000),
+                          rng.uniform(1, 7, 5000), rng.lognormal(2, 3, 5000)])
+    d = dev(pts)
+    for appr in (True, False):
+        got = host(bldm.psi(d, appr=appr))
+        ref = oracle.psi_array(pts, appr=appr)
+        err = np.abs(got - ref) / np.maximum(1.0, np.abs(ref))
+        assert err.max() <= 2e-14, (appr, err.max(), pts[err.argmax()])
+
+
+def test_psi_f32(bldm):
+    from scipy.special import digamma
+    rng = np.random.default_rng(1)
+    pts = np.concatenate([rng.uniform(1, 7, 4000), rng.lognormal(2, 3, 4000)]).astype(np.float32)
+    got = host(bldm.psi(dev(pts, torch.float32))).astype(np.float64)
+    ref = digamma(pts.astype(np.float64))
+    assert (np.abs(got - ref) / np.maximum(1.0, np.abs(ref))).max() <= 2e-6
+
+
+# ------------------------------------------------- per-stage (reference funcs tests)
+def test_tensor_sums_stage(bldm, oracle, is_approx):
+    rng = np.random.default_rng(2)
+    S = rng.uniform(-1, 1, (1024, 456, 17))       # Eigen setRandom range
+    pjk, ipk, ijp = (host(t) for t in bldm.tensor_sums(dev(S)))
+    rp, ri, rj = oracle.tensor_sums(S)
+    assert is_approx(pjk, rp, 1e-12) and is_approx(ipk, ri, 1e-12) and is_approx(ijp, rj, 1e-12)
+
+
+@pytest.mark.parametrize("appr", [True, False])
+def test_grad_plus_stage(bldm, oracle, is_approx, appr):
+    rng = np.random.default_rng(3)
+    x, y, z = 131, 456, 89
+    S = rng.uniform(-1, 1, (x, y, z)) + 1
+    beta_eph = rng.uniform(-1, 1, (y, z)) + 1
+    got = host(bldm.update_grad_plus(dev(S), dev(beta_eph), appr=appr))
+    ref = oracle.update_grad_plus(S, beta_eph, appr=appr)
+    assert is_approx(got, ref, 1e-12)
+
+
+def test_grad_minus_stage(bldm, oracle, is_approx):
+    rng = np.random.default_rng(4)
+    ae = rng.uniform(0.5, 20, (356, 17))
+    for appr in (True, False):
+        got = host(bldm.update_grad_minus(dev(ae), appr=appr))
+        assert is_approx(got, oracle.update_grad_minus(ae, appr=appr), 1e-12)
+
+
+def _nom_inputs(rng, x=356, y=478, z=17):
+    X = rng.uniform(-1, 1, (x, y)) + 10
+    Xr = 1.0 / X
+    gm = rng.uniform(-1, 1, (x, z)) + 2
+    S = rng.uniform(-1, 1, (x, y, z)) + 1
+    return X, Xr, gm, S
+
+
+def test_nom_stage(bldm, oracle, is_approx):
+    X, Xr, gm, S = _nom_inputs(np.random.default_rng(5))
+    got = host(bldm.update_nom(dev(Xr), dev(gm), dev(S)))
+    assert is_approx(got, oracle.update_nom(Xr, gm, S), 1e-12)
+
+
+def test_denom_stage(bldm, oracle, is_approx):
+    X, Xr, gm, S = _nom_inputs(np.random.default_rng(6))
+    gp = S.copy()
+    got = host(bldm.update_denom(dev(Xr), dev(gp), dev(S)))
+    assert is_approx(got, oracle.update_denom(Xr, gp, S), 1e-12)
+
+
+def test_update_S_stage(bldm, oracle, is_approx):
+    rng = np.random.default_rng(7)
+    X, Xr, gm, S = _nom_inputs(rng)
+    x, y, z = S.shape
+    nom = rng.uniform(-1, 1, (x, y)) + 3
+    den = rng.uniform(-1, 1, (x, y)) + 5
+    gp = S.copy()
+    ijp = S.sum(2)
+    dS = dev(S)
+    bldm.update_S(dev(X), dev(nom), dev(den), dev(gm), dev(gp), dev(ijp), dS)
+    ref = oracle.update_S(X, nom, den, gm, gp, ijp, S)
+    assert is_approx(host(dS), ref, 1e-12)
+
+
+# ------------------------------------------------------------- fused solver
+def test_plain_small_golden_parity(bldm, plain_small_golden):
+    g = plain_small_golden
+    params = bldm.Params(5.0, 0.1, g["alpha"], g["beta"])
+    S = bldm.bld_mult(g["X"], 8, params, int(g["iters"]), use_psi_appr=True, S0=g["S0"])
+    assert rel_err(S, g["S"]) <= 1e-9
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_modes_match_oracle(bldm, oracle, workloads, mode):
+    prob = workloads.plain_small(5)
+    X, z = prob["X"], prob["z"]
+    S0 = oracle.init_S(X, z, 3)
+    ref = oracle.bld_mult(X, z, prob["alpha"], prob["beta"], 60, mode, 1e-50, S0=S0)
+    params = bldm.Params(prob["a"], prob["b"], prob["alpha"], prob["beta"])
+    S = bldm._solve(X, z, params, 60, mode, 1e-50, S0, 0, bldm.F64, None)
+    assert rel_err(S, ref) <= 1e-9
+
+
+SHAPES = [(1, 1, 1), (3, 5, 1), (2, 3, 2), (33, 65, 3), (65, 33, 17), (7, 300, 5),
+          (5, 7, 33), (40, 41, 64), (9, 13, 100), (4, 9, 128), (3, 5, 256), (2, 3, 255), (2, 3, 512),
+          (300, 7, 8), (17, 1000, 4)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_odd_shapes_fp64(bldm, oracle, shape):
+    x, y, z = shape
+    rng = np.random.default_rng(x * 1000003 + y * 101 + z)
+    X = rng.poisson(rng.uniform(0.2, 30), (x, y)).astype(np.float64)
+    alpha = rng.uniform(0.5, 2, x)
+    beta = rng.uniform(0.5, 2, z)
+    S0 = oracle.init_S(X, z, 1)
+    ref = oracle.bld_mult(X, z, alpha, beta, 12, oracle.PSI_APPR, 1e-50, S0=S0)
+    S = bldm.bld_mult(X, z, bldm.Params(1, 1, alpha, beta), 12, True, S0=S0)
+    assert rel_err(S, ref) <= 1e-9
+
+
+@pytest.mark.parametrize("shape", [(3, 5, 1), (33, 65, 3), (40, 41, 4), (9, 13, 64), (5, 7, 17),
+                                   (64, 48, 8), (4, 9, 512), (3, 4, 1000)])
+def test_odd_shapes_fp32(bldm, oracle, shape):
+    x, y, z = shape
+    rng = np.random.default_rng(x * 7 + y * 13 + z)
+    X = rng.poisson(rng.uniform(0.5, 20), (x, y)).astype(np.float64)
+    alpha, beta = np.ones(x), np.ones(z)
+    S0 = oracle.init_S(X, z, 2)
+    ref = oracle.bld_mult(X, z, alpha, beta, 12, oracle.PSI_APPR, 1e-50, S0=S0)
+    S = bldm.bld_mult(X, z, bldm.Params(1, 1, alpha, beta), 12, True,
+                      S0=S0.astype(np.float32), dtype=bldm.F32)
+    # FP32 storage: 12 iterations stay within 1e-5 (max-norm relative) of FP64
+    assert rel_err(S, ref) <= 1e-5
+
+
+def test_fp32_plain_small_vs_fp64_oracle(bldm, plain_small_golden):
+    g = plain_small_golden
+    params = bldm.Params(5.0, 0.1, g["alpha"], g["beta"])
+    S = bldm.bld_mult(g["X"], 8, params, int(g["iters"]), use_psi_appr=True,
+                      S0=g["S0"].astype(np.float32), dtype=bldm.F32)
+    assert np.all(np.isfinite(S))
+    # 200 iterations in FP32 with compensated sums: 1e-4 max-norm relative
+    assert rel_err(S, g["S"]) <= 1e-4
+
+
+def test_zero_X_gives_zero_S(bldm):
+    for dt in (bldm.F64, bldm.F32):
+        S = bldm.bld_mult_cuda(np.zeros((8, 10)), 3, bldm.Params.from_shape((8, 10, 3)), 1000,
+                               dtype=dt)
+        assert np.all(S == 0)
+
+
+def test_zero_rows_cols_and_inconsistent_S0(bldm, oracle):
+    rng = np.random.default_rng(9)
+    X = rng.poisson(4.0, (20, 30)).astype(float)
+    X[3, :] = 0
+    X[:, 7] = 0
+    S0 = oracle.init_S(X, 6, 5)
+    S0[1, 2, :] = 0.0          # X > 0 but the initial fiber is empty
+    S0[3, 4, :] = 1.0          # X == 0 but the initial fiber is not
+    a, b = np.ones(20), np.ones(6)
+    ref = oracle.bld_mult(X, 6, a, b, 20, oracle.PSI_APPR, 1e-50, S0=S0)
+    S = bldm.bld_mult(X, 6, bldm.Params(1, 1, a, b), 20, True, S0=S0)
+    assert np.all(np.isfinite(S))
+    assert np.all(S[3] == 0) and np.all(S[:, 7] == 0) and np.all(S[1, 2] == 0)
+    assert rel_err(S, ref) <= 1e-9
+    S32 = bldm.bld_mult(X, 6, bldm.Params(1, 1, a, b), 20, True, S0=S0.astype(np.float32),
+                        dtype=bldm.F32)
+    assert np.all(np.isfinite(S32)) and np.all(S32[3] == 0) and np.all(S32[1, 2] == 0)
+
+
+def test_solver_is_deterministic(bldm, workloads):
+    prob = workloads.plain_small(1)
+    params = bldm.Params(prob["a"], prob["b"], prob["alpha"], prob["beta"])
+    a = bldm.bld_mult_cuda(prob["X"], prob["z"], params, 50, True, seed=4)
+    b = bldm.bld_mult_cuda(prob["X"], prob["z"], params, 50, True, seed=4)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_device_init_S_matches_oracle(bldm, oracle):
+    rng = np.random.default_rng(10)
+    X = rng.poisson(5.0, (50, 70)).astype(float)
+    plan = bldm.Plan(50, 70, 9)
+    dX = dev(X)
+    dS = torch.empty((50, 70, 9), dtype=torch.float64, device="cuda")
+    plan.init_S(dX, dS, seed=77)
+    got = host(dS)
+    ref = oracle.init_S(X, 9, 77)
+    assert rel_err(got, ref) <= 1e-14
+    # a solve with S0=None starts from the same tensor
+    params = bldm.Params(1, 1, np.ones(50), np.ones(9))
+    S1 = bldm.bld_mult(X, 9, params, 3, True, seed=77)
+    S2 = bldm.bld_mult(X, 9, params, 3, True, S0=ref)
+    assert rel_err(S1, S2) <= 1e-13
+    plan.close()
+
+
+def test_plan_api_matches_host_api(bldm, workloads, oracle):
+    prob = workloads.plain_small(2)
+    X, z = prob["X"], prob["z"]
+    x, y = X.shape
+    S0 = oracle.init_S(X, z, 8)
+    params = bldm.Params(prob["a"], prob["b"], prob["alpha"], prob["beta"])
+    ref = bldm.bld_mult(X, z, params, 40, True, S0=S0)
+    plan = bldm.Plan(x, y, z)
+    dS = dev(S0)
+    plan.run(dev(X), dev(prob["alpha"]), dev(prob["beta"]), dS, 40, bldm.PSI_APPR)
+    plan.check()
+    np.testing.assert_array_equal(host(dS), ref)
+    assert plan.launch_count() == 2 + 40 + 39
+    assert plan.workspace_bytes() > 0
+    plan.close()
+
+
+def test_full_size_one_iteration_parity(bldm, oracle, workloads):
+    prob = workloads.plain_large(1)
+    X, z = prob["X"], prob["z"]
+    oracle.set_threads(0)
+    S0 = oracle.init_S(X, z, 0)
+    ref = oracle.bld_mult(X, z, prob["alpha"], prob["beta"], 1, oracle.PSI_APPR, 1e-50, S0=S0)
+    params = bldm.Params(prob["a"], prob["b"], prob["alpha"], prob["beta"])
+    S = bldm.bld_mult(X, z, params, 1, True, S0=S0)
+    assert rel_err(S, ref) <= 1e-12
+    # size-independent properties after more iterations: nonnegative, finite,
+    # zero fibers of X stay zero, the row sums move toward X
+    S5 = bldm.bld_mult(X, z, params, 5, True, S0=S0)
+    assert np.all(np.isfinite(S5)) and S5.min() >= 0
+    assert np.all(S5[X == 0] == 0)
+
+
+def test_log_marginal_device_matches_oracle(bldm, oracle):
+    rng = np.random.default_rng(11)
+    x, y, z = 70, 90, 12
+    S = rng.poisson(1.5, (x, y, z)).astype(float) * rng.random((x, y, z))
+    alpha = rng.uniform(0.5, 2, x)
+    beta = rng.uniform(0.5, 2, z)
+    params = bldm.Params(3.0, 0.5, alpha, beta)
+    ref = oracle.log_marginal_S(S, alpha, beta, 3.0, 0.5)
+    got = bldm.log_marginal_S(dev(S), params)
+    assert abs(got - ref) <= 1e-11 * abs(ref)
+    got32 = bldm.log_marginal_S(dev(S, torch.float32), params, dtype=bldm.F32)
+    ref32 = oracle.log_marginal_S(S.astype(np.float32), alpha, beta, 3.0, 0.5)
+    assert abs(got32 - ref32) <= 1e-11 * abs(ref32)
+
+
+@pytest.mark.parametrize("use_appr", [False, True])
+def test_kat_8x10_on_gpu(bldm, oracle, kat, is_approx, use_appr):
+    X, z = kat["X"], kat["z"]
+    x = X.shape[0]
+    params = bldm.Params(kat["a"], kat["b"], np.ones(x), np.ones(z))
+    S = bldm.bld_mult(X, z, params, kat["iters"], use_appr, seed=kat["init_seed"])
+    name = "appr" if use_appr else "exact"
+    assert oracle.log_marginal_S(S, np.ones(x), np.ones(z), kat["a"], kat["b"]) >= -262
+    assert oracle.sparseness(S) >= kat["sparseness_min"]
+    assert is_approx(X, S.sum(2), kat["rowsum_isapprox_" + name])
+    assert rel_err(S.reshape(-1), kat["S_" + name]) <= 1e-9
