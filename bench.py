@@ -320,6 +320,29 @@ def run_ours(args):
     return 0
 
 
+def run_profile(args):
+    """One untimed solve of --profile-iters iterations (for ncu captures)."""
+    import torch
+    pkg = load_package()
+    import bnmf_algs_b200.workloads as W
+    x, y, z = (int(v) for v in args.shape.split("x"))
+    rng = np.random.default_rng(1)
+    X = W.allocation_model_X(x, y, z, 5.0, 0.01 if x * y >= 1 << 20 else 0.1, rng)
+    f64 = args.dtype == "f64"
+    dt_t = torch.float64 if f64 else torch.float32
+    dX = torch.as_tensor(X).to("cuda", dt_t)
+    dalpha = torch.ones(x, dtype=torch.float64, device="cuda")
+    dbeta = torch.ones(z, dtype=torch.float64, device="cuda")
+    dS = torch.empty((x, y, z), dtype=dt_t, device="cuda")
+    plan = pkg.Plan(x, y, z, pkg.F64 if f64 else pkg.F32)
+    plan.init_S(dX, dS, seed=0)
+    plan.run(dX, dalpha, dbeta, dS, args.profile_iters, pkg.PSI_APPR, 1e-50)
+    plan.check()
+    plan.close()
+    print(f"profile run ok: {x}x{y}x{z} {args.dtype}, {args.profile_iters} iterations")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -329,7 +352,15 @@ def main():
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="untimed: set up the workload, run --profile-iters iterations, exit "
+                         "(the command profiled by ncu)")
+    ap.add_argument("--profile-iters", type=int, default=3)
+    ap.add_argument("--shape", default="1024x1024x64",
+                    help="x*y*z of the plain workload for --profile-run")
     args = ap.parse_args()
+    if args.profile_run:
+        return run_profile(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
