@@ -116,6 +116,145 @@ __device__ __forceinline__ double psi_mode_f64(double v, bool appr) {
 }
 
 // ---------------------------------------------------------------------------
+// Throughput versions for the fused sweep, where FP64 issue slots bound the
+// kernel.  Same mathematical functions as above; only the evaluation differs.
+// ---------------------------------------------------------------------------
+
+// 1/d by two Newton-Raphson steps y <- y (2 - d y) from the hardware
+// reciprocal approximation (each step squares the relative error, so a seed
+// good to 2^-16 is already below double rounding after two steps).  Normal
+// finite d only (the seed flushes subnormals).
+__device__ __forceinline__ double rcp_nr(double d) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+    double e = fma(-d, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-d, y, 1.0);
+    return fma(y, e, y);
+}
+
+// Natural logarithm by the table-driven method of P. T. P. Tang ("Table-driven
+// implementation of the logarithm function in IEEE floating-point
+// arithmetic", ACM TOMS 16(4), 1990): x = 2^e m, m in [1,2); R_j = 1/c_j with
+// c_j = 1 + j/128 the nearest of 129 breakpoints; r = m R_j - 1 (one fused
+// rounding), |r| <= 2^-8; ln x = e ln2 + ln(1/R_j) + log1p(r) with log1p as
+// its Taylor series to r^6 (remainder below 2^-59).  ln2 is split in a
+// 32-bit-exact high part and a low part so that e*ln2_hi is exact.
+constexpr int kLogTabN = 129;
+constexpr double kLn2Hi = 6.93147180369123816490e-01;  // ln2 to 32 significant bits
+constexpr double kLn2Lo = 1.90821492927058770002e-10;  // ln2 - kLn2Hi
+
+// Fills tab[j] = {ln(1/R_j), R_j}; call once per CTA before use.
+__device__ __forceinline__ void log_tab_init(double2* tab, int tid, int nthreads) {
+    for (int j = tid; j < kLogTabN; j += nthreads) {
+        const double R = 1.0 / (1.0 + double(j) * (1.0 / 128.0));
+        tab[j] = make_double2(-log(R), R);
+    }
+}
+
+__device__ __forceinline__ double log_tab(double x, const double2* tab) {
+    if (!(x >= 2.2250738585072014e-308 && x <= 1.7976931348623157e308)) return log(x);
+    const long long b = __double_as_longlong(x);
+    const int ex = int(b >> 52) - 1023;
+    const long long mb = (b & 0x000FFFFFFFFFFFFFll) | 0x3FF0000000000000ll;
+    const double m = __longlong_as_double(mb);
+    const int j = (int((mb >> 44) & 0xFF) + 1) >> 1;  // nearest breakpoint, 0..128
+    const double2 t = tab[j];
+    const double r = fma(m, t.y, -1.0);
+    double q = fma(r, -1.0 / 6.0, 1.0 / 5.0);
+    q = fma(q, r, -1.0 / 4.0);
+    q = fma(q, r, 1.0 / 3.0);
+    q = fma(q, r, -1.0 / 2.0);
+    const double l1 = fma(q, r * r, r);
+    const double de = double(ex);
+    return fma(de, kLn2Hi, t.x) + fma(de, kLn2Lo, l1);
+}
+
+// Reciprocal used by the update: Newton-Raphson in FP64, IEEE in FP32.
+template <typename T> struct Rcp;
+template <> struct Rcp<double> {
+    __device__ __forceinline__ static double of(double d) {
+        const double a = fabs(d);
+        return (a >= 2.2250738585072014e-308 && a <= 4.49423283715578976932e307) ? rcp_nr(d)
+                                                                                 : 1.0 / d;
+    }
+};
+template <> struct Rcp<float> {
+    __device__ __forceinline__ static float of(float d) { return 1.0f / d; }
+};
+
+// psi(arg) for the NE elements of one pass, every lane of the warp together.
+template <int NE>
+__device__ __forceinline__ void psi_appr_batch(const double (&x)[NE], double (&out)[NE],
+                                               const double2* ltab) {
+    int n[NE];
+    double num[NE], den[NE];
+    bool six = false;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        n[e] = (x[e] < 1.0) ? 6 : ((x[e] < 6.0) ? 6 - __double2int_rz(x[e]) : 0);
+        six |= n[e] == 6;
+        num[e] = 0.0;
+        den[e] = 1.0;
+    }
+    // Arguments >= 1 need at most five unit shifts; a sixth (argument < 1,
+    // i.e. S < 0) is taken only when some lane of the warp needs it.
+    const int steps = __any_sync(0xffffffffu, six) ? 6 : 5;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        if (m == 5 && steps == 5) break;
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            const bool act = m < n[e];
+            const double f = act ? x[e] + double(m) : 1.0;
+            num[e] = act ? fma(num[e], f, den[e]) : num[e];
+            den[e] *= f;
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        const double xs = x[e] + double(n[e]);
+        const double inv = Rcp<double>::of(xs * den[e]);
+        const double r = den[e] * inv;
+        const double shift = num[e] * xs * inv;
+        const double r2 = r * r;
+        double t = fma(r2, -1.0 / 12.0, 691.0 / 32760.0);
+        t = fma(r2, -t, 1.0 / 132.0);
+        t = fma(r2, -t, 1.0 / 240.0);
+        t = fma(r2, -t, 1.0 / 252.0);
+        t = fma(r2, -t, 1.0 / 120.0);
+        t = fma(r2, -t, 1.0 / 12.0);
+        out[e] = log_tab(xs, ltab) - 0.5 * r - r2 * t - shift;
+    }
+}
+
+template <typename T, bool APPR> struct PsiPass;
+template <> struct PsiPass<double, true> {
+    template <int NE>
+    __device__ __forceinline__ static void run(const double (&x)[NE], double (&out)[NE],
+                                               const double2* ltab) {
+        psi_appr_batch<NE>(x, out, ltab);
+    }
+};
+template <> struct PsiPass<double, false> {
+    template <int NE>
+    __device__ __forceinline__ static void run(const double (&x)[NE], double (&out)[NE],
+                                               const double2*) {
+#pragma unroll
+        for (int e = 0; e < NE; ++e) out[e] = psi_exact_f64(x[e]);
+    }
+};
+template <bool APPR> struct PsiPass<float, APPR> {
+    template <int NE>
+    __device__ __forceinline__ static void run(const float (&x)[NE], float (&out)[NE],
+                                               const double2*) {
+#pragma unroll
+        for (int e = 0; e < NE; ++e) out[e] = psi_f32(x[e]);
+    }
+};
+
+
+// ---------------------------------------------------------------------------
 // Timers, bounded waits, bulk copies.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long global_ns() {

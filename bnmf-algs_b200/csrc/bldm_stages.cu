@@ -110,7 +110,20 @@ __global__ void update_S_kernel(const double* X, const double* nom, const double
 }
 
 __global__ void psi_f64_kernel(const double* in, long long n, int appr, double* out) {
+    __shared__ double2 ltab[kLogTabN];
+    if (appr == 2) {
+        log_tab_init(ltab, threadIdx.x, kT);
+        __syncthreads();
+    }
     const long long e = (long long)blockIdx.x * kT + threadIdx.x;
+    if (appr == 2) {
+        // the fused sweep's evaluation (all lanes take part)
+        const double xv[1] = {e < n ? in[e] : 1.0};
+        double r[1];
+        psi_appr_batch<1>(xv, r, ltab);
+        if (e < n) out[e] = r[0];
+        return;
+    }
     if (e < n) out[e] = appr ? psi_appr_f64(in[e]) : psi_exact_f64(in[e]);
 }
 __global__ void psi_f32_kernel(const float* in, long long n, float* out) {

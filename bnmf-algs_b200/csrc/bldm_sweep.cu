@@ -119,8 +119,10 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
         for (int s = 0; s < p.stages; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
+    __shared__ double2 ltab[kLogTabN];  // ln table of the FP64 digamma
     if (UPDATE) {
         for (long long k = tid; k < z; k += kSweepThreads) sAS[k] = p.psiAS[k];
+        if (sizeof(T) == 8 && APPR) log_tab_init(ltab, tid, kSweepThreads);
     }
     __syncthreads();
 
@@ -213,74 +215,101 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
             for (int v = 0; v < VEC; ++v) ip[m][v].init();
 
         if (ok) {
+            T sv[CPW][MCH][VEC];
+            T xv[CPW];
 #pragma unroll
             for (int c = 0; c < CPW; ++c) {
                 const int jl = (warp * CPW + c) * FPW + g;
                 const bool fv = jl < cw;
-                T sv[MCH][VEC];
 #pragma unroll
                 for (int m = 0; m < MCH; ++m) {
                     const long long k0 = (long long)(m * LPF + q) * VEC;
                     // VEC > 1 only when z*sizeof(T) is a multiple of 16, so a
                     // chunk is entirely inside or entirely outside the fiber.
                     if (fv && k0 < z) {
-                        VecIO<T, VEC>::load(sS + (long long)jl * z + k0, sv[m]);
+                        VecIO<T, VEC>::load(sS + (long long)jl * z + k0, sv[c][m]);
                     } else {
 #pragma unroll
-                        for (int v = 0; v < VEC; ++v) sv[m][v] = T(0);
+                        for (int v = 0; v < VEC; ++v) sv[c][m][v] = T(0);
                     }
                 }
-                if (UPDATE) {
-                    const T xv = fv ? sX[jl] : T(0);
-                    T gp[MCH][VEC];
-                    T as = T(0), an = T(0), ad = T(0);
+                xv[c] = (UPDATE && fv) ? sX[jl] : T(0);
+            }
+            if (UPDATE) {
+                const T teps = T(p.eps);
 #pragma unroll
-                    for (int m = 0; m < MCH; ++m)
+                for (int c = 0; c < CPW; ++c) {
+                    const int jl = (warp * CPW + c) * FPW + g;
+                    const bool fv = jl < cw;
+                    T sn[MCH][VEC];
+                    // A fiber with X == 0 updates to zero whatever its digamma
+                    // values (the reference formula multiplies by X/(S_ijp+eps));
+                    // a pass whose fibers all have X == 0 skips the arithmetic.
+                    if (__any_sync(0xffffffffu, xv[c] != T(0))) {
+                        T arg[MCH * VEC], ps[MCH * VEC];
 #pragma unroll
-                        for (int v = 0; v < VEC; ++v) {
-                            const T e = sv[m][v];
-                            const T ps = APPR ? Psi<T>::appr(e + T(1)) : Psi<T>::exact(e + T(1));
-                            gp[m][v] = pB[c][m][v] - ps;
-                            as += e;
-                            an += e * gm[m][v];
-                            ad += e * gp[m][v];
-                        }
-                    as = group_sum<LPF>(as);
-                    an = group_sum<LPF>(an);
-                    ad = group_sum<LPF>(ad);
-                    const T teps = T(p.eps);
-                    const T xr = T(1) / (xv + teps);
-                    const T nom = an * xr;
-                    const T den = ad * xr;
-                    const T xos = xv / (as + teps);
-                    // X == 0 (or an all-zero fiber) keeps the fiber at zero, which is
-                    // what the reference formula yields in FP64; it also avoids the
-                    // 0 * inf of FP32, where eps = 1e-50 underflows to zero.
-                    const bool zero = (xv == T(0)) || (as == T(0));
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) arg[m * VEC + v] = sv[c][m][v] + T(1);
+                        PsiPass<T, APPR>::template run<MCH * VEC>(arg, ps, ltab);
+                        T gp[MCH][VEC];
+                        T as = T(0), an = T(0), ad = T(0);
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) {
+                                const T e = sv[c][m][v];
+                                gp[m][v] = pB[c][m][v] - ps[m * VEC + v];
+                                as += e;
+                                an += e * gm[m][v];
+                                ad += e * gp[m][v];
+                            }
+                        as = group_sum<LPF>(as);
+                        an = group_sum<LPF>(an);
+                        ad = group_sum<LPF>(ad);
+                        const T xr = T(1) / (xv[c] + teps);
+                        const T nom = an * xr;
+                        const T den = ad * xr + teps;
+                        const T xos = xv[c] / (as + teps);
+                        // X == 0 (or an all-zero fiber) keeps the fiber at zero: the
+                        // reference's FP64 result, and no 0 * inf in FP32 where
+                        // eps = 1e-50 underflows to zero.
+                        const bool zero = (xv[c] == T(0)) || (as == T(0));
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v)
+                                sn[m][v] = zero ? T(0)
+                                                : sv[c][m][v] * (((gp[m][v] + nom) * xos) *
+                                                                 Rcp<T>::of(gm[m][v] + den));
+                    } else {
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) sn[m][v] = T(0);
+                    }
 #pragma unroll
                     for (int m = 0; m < MCH; ++m) {
-                        T sn[VEC];
 #pragma unroll
                         for (int v = 0; v < VEC; ++v) {
-                            sn[v] = zero ? T(0)
-                                         : sv[m][v] * (((gp[m][v] + nom) * xos) /
-                                                       (gm[m][v] + den + teps));
-                            pj[c][m][v].add(sn[v]);
-                            ip[m][v].add(sn[v]);
+                            pj[c][m][v].add(sn[m][v]);
+                            ip[m][v].add(sn[m][v]);
                         }
                         const long long k0 = (long long)(m * LPF + q) * VEC;
                         if (fv && k0 < z)
-                            VecIO<T, VEC>::store(p.S + ((i * p.y + c0 + jl) * z + k0), sn);
+                            VecIO<T, VEC>::store(p.S + ((i * p.y + c0 + jl) * z + k0), sn[m]);
                     }
-                } else {
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < CPW; ++c)
 #pragma unroll
                     for (int m = 0; m < MCH; ++m)
 #pragma unroll
                         for (int v = 0; v < VEC; ++v) {
-                            pj[c][m][v].add(sv[m][v]);
-                            ip[m][v].add(sv[m][v]);
+                            pj[c][m][v].add(sv[c][m][v]);
+                            ip[m][v].add(sv[c][m][v]);
                         }
-                }
             }
         }
 
@@ -521,7 +550,7 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
     c.capA = uint32_t(align_up(z * es + 32, 16));
     c.stage_bytes = c.capS + c.capX + c.capA;
     const size_t fixed = 64 + 2 * size_t(kSweepWarps) * z * 8 + z * es + 128;
-    const size_t budget = 110 * 1024;
+    const size_t budget = 106 * 1024;  // dynamic; + 2 KB static log table per CTA
     long st = budget > fixed ? long((budget - fixed) / c.stage_bytes) : 0;
     st = std::min(8L, st);
     if (st < 2) {
@@ -532,7 +561,7 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
     c.stages = int(st);
     c.smem_update = size_t(c.stages) * c.stage_bytes + fixed;
     c.smem_sums = c.smem_update;
-    c.ctas_per_sm = c.smem_update + 1024 <= 228 * 1024 / 2 ? 2 : 1;
+    c.ctas_per_sm = c.smem_update + 1024 + 16 * kLogTabN <= 228 * 1024 / 2 ? 2 : 1;
     // Row ranges: fill the resident CTA slots in one wave (a partial second
     // wave of a bandwidth-bound sweep costs a whole tail).
     const long target = long(c.ctas_per_sm) * num_sms;

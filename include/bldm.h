@@ -190,7 +190,9 @@ int bldm_update_S_f64(const double* d_X, const double* d_nom,
                       const double* d_grad_plus, const double* d_S_ijp,
                       size_t x, size_t y, size_t z, double eps, double* d_S,
                       void* stream);
-/* util::psi_appr / exact digamma over an array (appr != 0: psi_appr). */
+/* util::psi_appr / exact digamma over an array: appr == 0 exact, 1 psi_appr,
+ * 2 psi_appr as evaluated inside the fused sweep (same function, batched
+ * form with Newton-Raphson reciprocals and a table logarithm). */
 int bldm_psi_f64(const double* d_in, size_t n, int appr, double* d_out, void* stream);
 int bldm_psi_f32(const float* d_in, size_t n, float* d_out, void* stream);
 

@@ -38,11 +38,12 @@ def test_psi_appr_and_exact_match_oracle(bldm, oracle, psi_points):
     pts = np.concatenate([psi_points["points"], rng.uniform(1e-6, 1, 5000),
                           rng.uniform(1, 7, 5000), rng.lognormal(2, 3, 5000)])
     d = dev(pts)
-    for appr in (True, False):
-        got = host(bldm.psi(d, appr=appr))
-        ref = oracle.psi_array(pts, appr=appr)
+    # 0: exact, 1: psi_appr, 2: psi_appr as the fused sweep evaluates it
+    for mode in (0, 1, 2):
+        got = host(bldm.psi(d, appr=mode))
+        ref = oracle.psi_array(pts, appr=mode != 0)
         err = np.abs(got - ref) / np.maximum(1.0, np.abs(ref))
-        assert err.max() <= 2e-14, (appr, err.max(), pts[err.argmax()])
+        assert err.max() <= 2e-14, (mode, err.max(), pts[err.argmax()])
 
 
 def test_psi_f32(bldm):
