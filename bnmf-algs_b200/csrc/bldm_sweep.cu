@@ -32,7 +32,8 @@ constexpr int kSweepWarps = 8;
 constexpr int kSweepThreads = kSweepWarps * 32;
 constexpr int kFinThreads = 256;
 
-__host__ __device__ constexpr int cpw_for(int ev) { return ev <= 2 ? 4 : (ev <= 4 ? 2 : 1); }
+// fiber passes per warp per row, from the bytes a lane holds per fiber
+__host__ __device__ constexpr int cpw_for(int bytes) { return bytes <= 16 ? 4 : (bytes <= 32 ? 2 : 1); }
 
 template <typename T> struct SweepParams {
     T* S;
@@ -93,7 +94,7 @@ template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR>
 __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepParams<T> p) {
     constexpr int NW = kSweepWarps;
     constexpr int FPW = 32 / LPF;
-    constexpr int CPW = cpw_for(MCH * VEC);
+    constexpr int CPW = cpw_for(MCH * VEC * int(sizeof(T)));
     extern __shared__ __align__(128) unsigned char smem[];
 
     const int tid = threadIdx.x;
@@ -112,13 +113,15 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
 
     unsigned char* stage0 = smem;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)p.stages * p.stage_bytes);
-    double* red = reinterpret_cast<double*>(bars + 8);  // [2][NW][z]
-    T* sAS = reinterpret_cast<T*>(red + 2 * NW * z);   // [z]
+    double* red = reinterpret_cast<double*>(bars + 8);         // [stages][NW][z]
+    T* sAS = reinterpret_cast<T*>(red + (size_t)p.stages * NW * z);  // [z]
+    __shared__ int cnt[8];  // per-stage arrivals of warps (monotonic)
 
     if (tid == 0) {
         for (int s = 0; s < p.stages; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
+    if (tid < 8) cnt[tid] = 0;
     __shared__ double2 ltab[kLogTabN];  // ln table of the FP64 digamma
     if (UPDATE) {
         for (long long k = tid; k < z; k += kSweepThreads) sAS[k] = p.psiAS[k];
@@ -188,6 +191,17 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
         // warp-uniform: the lane-group shuffles below need every lane of the warp
         const bool ok =
             __all_sync(0xffffffffu, mbar_wait_bounded(&bars[s], (uint32_t)((t / p.stages) & 1)));
+        if (!ok) {
+            // Give up: flag the error and wait (bounded) for the copies that
+            // may still be landing in this CTA's shared memory.
+            if (lane == 0) {
+                atomicOr(p.err, DEV_ERR_WAIT_TIMEOUT);
+                const int issued = min(nrows, t + p.stages);
+                for (int u = t; u < issued; ++u)
+                    (void)mbar_wait_bounded(&bars[u % p.stages], (uint32_t)((u / p.stages) & 1));
+            }
+            return;
+        }
         const long long i = r0 + t;
         const unsigned char* st = stage0 + (size_t)s * p.stage_bytes;
         const uintptr_t aS = reinterpret_cast<uintptr_t>(p.S + (i * p.y + c0) * z);
@@ -313,8 +327,8 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
             }
         }
 
-        // S_ipk partial of row i over this band: fiber slots -> warps -> CTA.
-        double* redb = red + (size_t)(t & 1) * NW * z;
+        // S_ipk partial of row i over this band: fiber slots -> warp -> red[s][warp].
+        double* redw = red + ((size_t)s * NW + warp) * z;
 #pragma unroll
         for (int m = 0; m < MCH; ++m)
 #pragma unroll
@@ -322,25 +336,31 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
                 double val = ip[m][v].value();
                 if (FPW > 1) val = cross_group_sum<LPF>(val);
                 const long long k = (long long)(m * LPF + q) * VEC + v;
-                if (g == 0 && k < z) redb[(size_t)warp * z + k] = val;
+                if (g == 0 && k < z) redw[k] = val;
             }
-        const int all_ok = __syncthreads_and(ok ? 1 : 0);
-        if (!all_ok) {
-            if (tid == 0) {
-                atomicOr(p.err, DEV_ERR_WAIT_TIMEOUT);
-                const int issued = min(nrows, t + p.stages);
-                for (int u = t; u < issued; ++u)
-                    (void)mbar_wait_bounded(&bars[u % p.stages], (uint32_t)((u / p.stages) & 1));
-            }
-            return;
+        __syncwarp();
+        // No CTA barrier per row: each warp counts itself done with stage s;
+        // the last of the NW warps (the count reaches a multiple of NW) adds the
+        // warps' partials in warp order, writes the S_ipk partial of row i and
+        // refills the stage.  Warps drift apart by up to `stages` rows.
+        int last = 0;
+        if (lane == 0) {
+            __threadfence_block();
+            last = (atomicAdd(&cnt[s], 1) == (t / p.stages + 1) * NW - 1) ? 1 : 0;
         }
-        for (long long k = tid; k < z; k += kSweepThreads) {
-            double sum = 0.0;
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last) {
+            __threadfence_block();
+            const double* reds = red + (size_t)s * NW * z;
+            for (long long k = lane; k < z; k += 32) {
+                double sum = 0.0;
 #pragma unroll
-            for (int w = 0; w < NW; ++w) sum += redb[(size_t)w * z + k];
-            p.part_ipk[((long long)band * p.x + i) * z + k] = sum;
+                for (int w = 0; w < NW; ++w) sum += reds[(size_t)w * z + k];
+                p.part_ipk[((long long)band * p.x + i) * z + k] = sum;
+            }
+            __syncwarp();
+            if (lane == 0 && t + p.stages < nrows) issue(t + p.stages);
         }
-        if (tid == 0 && t + p.stages < nrows) issue(t + p.stages);
     }
 
     // S_pjk partial of the band over this CTA's rows: each (j,k) has one owner.
@@ -540,7 +560,7 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
         c.mch = pow2ceil((nch + 31) / 32);
         if (c.mch > 8) return BLDM_ERR_UNSUPPORTED;
     }
-    c.cpw = cpw_for(c.mch * c.vec);
+    c.cpw = cpw_for(int(c.mch * c.vec * es));
     c.warps = kSweepWarps;
     const int fpw = 32 / c.lpf;
     c.band_w = c.warps * c.cpw * fpw;
@@ -549,17 +569,19 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
     c.capX = uint32_t(align_up(size_t(c.band_w) * es + 32, 16));
     c.capA = uint32_t(align_up(z * es + 32, 16));
     c.stage_bytes = c.capS + c.capX + c.capA;
-    const size_t fixed = 64 + 2 * size_t(kSweepWarps) * z * 8 + z * es + 128;
+    // each stage also owns a [warps][z] slice of S_ipk partials (FP64)
+    const size_t per_stage = c.stage_bytes + size_t(kSweepWarps) * z * 8;
+    const size_t fixed = 64 + z * es + 128;
     const size_t budget = 106 * 1024;  // dynamic; + 2 KB static log table per CTA
-    long st = budget > fixed ? long((budget - fixed) / c.stage_bytes) : 0;
+    long st = budget > fixed ? long((budget - fixed) / per_stage) : 0;
     st = std::min(8L, st);
     if (st < 2) {
         // large slabs: allow one CTA per SM
-        st = std::min(8L, long((220 * 1024 - fixed) / c.stage_bytes));
+        st = std::min(8L, long((220 * 1024 - fixed) / per_stage));
         if (st < 2) return BLDM_ERR_UNSUPPORTED;
     }
     c.stages = int(st);
-    c.smem_update = size_t(c.stages) * c.stage_bytes + fixed;
+    c.smem_update = size_t(c.stages) * per_stage + fixed;
     c.smem_sums = c.smem_update;
     c.ctas_per_sm = c.smem_update + 1024 + 16 * kLogTabN <= 228 * 1024 / 2 ? 2 : 1;
     // Row ranges: fill the resident CTA slots in one wave (a partial second
