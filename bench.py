@@ -343,6 +343,54 @@ def run_profile(args):
     return 0
 
 
+def make_X(kind, x, y, z, rng):
+    """X kinds: 'model' (the plain workload's allocation-model draw), 'dense'
+    (1 + Poisson(10), no zeros), 'zeros' (all zero)."""
+    load_package()
+    import bnmf_algs_b200.workloads as W
+    if kind == "model":
+        return W.allocation_model_X(x, y, z, 5.0, 0.01, rng)
+    if kind == "dense":
+        return 1.0 + rng.poisson(10.0, (x, y)).astype(np.float64)
+    return np.zeros((x, y))
+
+
+def run_kernel_matrix(args):
+    import torch
+    pkg = load_package()
+    x, y, z = (int(v) for v in args.shape.split("x"))
+    peak, _ = hbm_peak()
+    knobs = [(0, 0, 0), (8, 1, 0), (3, 2, 0), (4, 2, 0), (2, 2, 0), (6, 1, 0)]
+    for dt in ("f64", "f32"):
+        f64 = dt == "f64"
+        es = 8 if f64 else 4
+        dt_t = torch.float64 if f64 else torch.float32
+        for kind in ("model", "dense", "zeros"):
+            X = make_X(kind, x, y, z, np.random.default_rng(1))
+            dX = torch.as_tensor(X).to("cuda", dt_t)
+            da = torch.ones(x, dtype=torch.float64, device="cuda")
+            db = torch.ones(z, dtype=torch.float64, device="cuda")
+            dS = torch.empty((x, y, z), dtype=dt_t, device="cuda")
+            for st, cps, rr in knobs:
+                try:
+                    plan = pkg.Plan(x, y, z, pkg.F64 if f64 else pkg.F32, st, cps, rr)
+                except Exception as e:
+                    print(json.dumps({"dtype": dt, "x_kind": kind, "knobs": [st, cps, rr],
+                                      "error": str(e)}))
+                    continue
+                plan.init_S(dX, dS, seed=0)
+                plan.run(dX, da, db, dS, 3, pkg.PSI_APPR)
+                kms, ims = plan.profile(dX, da, db, dS, 10, pkg.PSI_APPR)
+                alg = 2 * x * y * z * es + x * y * es
+                print(json.dumps({"dtype": dt, "x_kind": kind, "knobs": [st, cps, rr],
+                                  "tuning": plan.tuning(), "kernel_ms": round(kms, 4),
+                                  "iteration_ms": round(ims, 4),
+                                  "frac": round(alg / (kms / 1e3) / 1e9 / peak, 3)}), flush=True)
+                plan.close()
+            del dX, dS
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,10 +405,15 @@ def main():
                          "(the command profiled by ncu)")
     ap.add_argument("--profile-iters", type=int, default=3)
     ap.add_argument("--shape", default="1024x1024x64",
-                    help="x*y*z of the plain workload for --profile-run")
+                    help="x*y*z of the plain workload for --profile-run / --kernel-matrix")
+    ap.add_argument("--kernel-matrix", action="store_true",
+                    help="time the update sweep (CUDA events) over X kinds, dtypes and launch "
+                         "knobs; one JSON line each")
     args = ap.parse_args()
     if args.profile_run:
         return run_profile(args)
+    if args.kernel_matrix:
+        return run_kernel_matrix(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

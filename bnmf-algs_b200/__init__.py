@@ -61,6 +61,11 @@ class bldm_params(ctypes.Structure):
                 ("beta", ctypes.POINTER(ctypes.c_double)), ("n_beta", ctypes.c_size_t)]
 
 
+class bldm_tuning(ctypes.Structure):
+    _fields_ = [("stages", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("row_ranges", ctypes.c_int)]
+
+
 class bldm_stats(ctypes.Structure):
     _fields_ = [("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("iterations", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
@@ -104,6 +109,9 @@ SIGNATURES = {
                                       ctypes.POINTER(bldm_stats)]),
     "bldm_release_cache": (ctypes.c_int, []),
     "bldm_plan_create": (ctypes.c_int, [ctypes.POINTER(_vp), _sz, _sz, _sz, ctypes.c_int]),
+    "bldm_plan_create_tuned": (ctypes.c_int, [ctypes.POINTER(_vp), _sz, _sz, _sz, ctypes.c_int,
+                                              ctypes.POINTER(bldm_tuning)]),
+    "bldm_plan_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(bldm_tuning)]),
     "bldm_plan_destroy": (ctypes.c_int, [_vp]),
     "bldm_plan_workspace_bytes": (ctypes.c_int, [_vp, ctypes.POINTER(_sz)]),
     "bldm_plan_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _sz, ctypes.c_int, ctypes.c_double,
@@ -232,11 +240,21 @@ def _stream_ptr(stream):
 class Plan:
     """bldm_plan: workspace for one (x, y, z, dtype); runs on device tensors."""
 
-    def __init__(self, x, y, z, dtype=F64):
+    def __init__(self, x, y, z, dtype=F64, stages=0, ctas_per_sm=0, row_ranges=0):
         self._h = ctypes.c_void_p()
         self.shape = (x, y, z)
         self.dtype = dtype
-        _check(lib().bldm_plan_create(ctypes.byref(self._h), x, y, z, dtype), "plan_create")
+        if stages or ctas_per_sm or row_ranges:
+            t = bldm_tuning(int(stages), int(ctas_per_sm), int(row_ranges))
+            _check(lib().bldm_plan_create_tuned(ctypes.byref(self._h), x, y, z, dtype,
+                                                ctypes.byref(t)), "plan_create_tuned")
+        else:
+            _check(lib().bldm_plan_create(ctypes.byref(self._h), x, y, z, dtype), "plan_create")
+
+    def tuning(self):
+        t = bldm_tuning()
+        _check(lib().bldm_plan_get_tuning(self._h, ctypes.byref(t)))
+        return {"stages": t.stages, "ctas_per_sm": t.ctas_per_sm, "row_ranges": t.row_ranges}
 
     def close(self):
         if self._h:

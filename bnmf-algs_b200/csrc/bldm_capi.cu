@@ -238,6 +238,30 @@ int bldm_plan_create(bldm_plan** plan, size_t x, size_t y, size_t z, int dtype) 
     return BLDM_OK;
 }
 
+int bldm_plan_create_tuned(bldm_plan** plan, size_t x, size_t y, size_t z, int dtype,
+                           const bldm_tuning* tuning) {
+    if (!plan) return BLDM_ERR_BAD_ARG;
+    *plan = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return BLDM_ERR_NO_DEVICE;
+    std::unique_ptr<bldm_plan> p(new bldm_plan());
+    int rc = plan_setup(&p->impl, x, y, z, dtype, tuning);
+    if (rc) {
+        plan_free(&p->impl);
+        return rc;
+    }
+    *plan = p.release();
+    return BLDM_OK;
+}
+
+int bldm_plan_get_tuning(const bldm_plan* plan, bldm_tuning* out) {
+    if (!plan || !out) return BLDM_ERR_BAD_ARG;
+    out->stages = plan->impl.cfg.stages;
+    out->ctas_per_sm = plan->impl.cfg.ctas_per_sm;
+    out->row_ranges = plan->impl.cfg.n_rr;
+    return BLDM_OK;
+}
+
 int bldm_plan_destroy(bldm_plan* plan) {
     if (!plan) return BLDM_ERR_BAD_ARG;
     plan_free(&plan->impl);

@@ -133,6 +133,13 @@ __device__ __forceinline__ double rcp_nr(double d) {
     return fma(y, e, y);
 }
 
+// FP32 reciprocal: hardware approximation refined by one Newton-Raphson step.
+__device__ __forceinline__ float rcp_nr_f32(float d) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
+    return fmaf(y, fmaf(-d, y, 1.0f), y);
+}
+
 // Natural logarithm by the table-driven method of P. T. P. Tang ("Table-driven
 // implementation of the logarithm function in IEEE floating-point
 // arithmetic", ACM TOMS 16(4), 1990): x = 2^e m, m in [1,2); R_j = 1/c_j with
@@ -180,7 +187,10 @@ template <> struct Rcp<double> {
     }
 };
 template <> struct Rcp<float> {
-    __device__ __forceinline__ static float of(float d) { return 1.0f / d; }
+    __device__ __forceinline__ static float of(float d) {
+        const float a = fabsf(d);
+        return (a >= 1.17549435e-38f && a <= 8.5e37f) ? rcp_nr_f32(d) : 1.0f / d;
+    }
 };
 
 // psi(arg) for the NE elements of one pass, every lane of the warp together.
@@ -244,12 +254,54 @@ template <> struct PsiPass<double, false> {
         for (int e = 0; e < NE; ++e) out[e] = psi_exact_f64(x[e]);
     }
 };
+// FP32 digamma for the sweep: psi_f32's shift rule and series, with a
+// hardware reciprocal refined by one Newton-Raphson step and the hardware
+// base-2 logarithm (relative error about 2^-21, at the resolution of FP32 S).
+
+template <int NE>
+__device__ __forceinline__ void psi_f32_batch(const float (&x)[NE], float (&out)[NE]) {
+    int n[NE];
+    float num[NE], den[NE];
+    bool six = false;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        n[e] = (x[e] < 1.0f) ? 6 : ((x[e] < 6.0f) ? 6 - __float2int_rz(x[e]) : 0);
+        six |= n[e] == 6;
+        num[e] = 0.0f;
+        den[e] = 1.0f;
+    }
+    const int steps = __any_sync(0xffffffffu, six) ? 6 : 5;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        if (m == 5 && steps == 5) break;
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            const bool act = m < n[e];
+            const float f = act ? x[e] + float(m) : 1.0f;
+            num[e] = act ? fmaf(num[e], f, den[e]) : num[e];
+            den[e] *= f;
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        const float xs = x[e] + float(n[e]);
+        const float pd = xs * den[e];
+        const float inv = (pd >= 1.17549435e-38f && pd <= 8.5e37f) ? rcp_nr_f32(pd) : 1.0f / pd;
+        const float r = den[e] * inv;
+        const float shift = num[e] * xs * inv;
+        const float r2 = r * r;
+        float t = fmaf(r2, -1.f / 240.f, 1.f / 252.f);
+        t = fmaf(r2, -t, 1.f / 120.f);
+        t = fmaf(r2, -t, 1.f / 12.f);
+        out[e] = __logf(xs) - 0.5f * r - r2 * t - shift;
+    }
+}
+
 template <bool APPR> struct PsiPass<float, APPR> {
     template <int NE>
     __device__ __forceinline__ static void run(const float (&x)[NE], float (&out)[NE],
                                                const double2*) {
-#pragma unroll
-        for (int e = 0; e < NE; ++e) out[e] = psi_f32(x[e]);
+        psi_f32_batch<NE>(x, out);
     }
 };
 

@@ -56,7 +56,8 @@ struct PlanImpl {
 };
 
 // Implemented in bldm_sweep.cu.
-int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype);
+int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype,
+               const bldm_tuning* tune = nullptr);
 void plan_free(PlanImpl* p);
 int plan_run(PlanImpl* p, const void* dX, const double* dalpha, const double* dbeta,
              void* dS, size_t max_iter, int psi_mode, double eps, cudaStream_t st,

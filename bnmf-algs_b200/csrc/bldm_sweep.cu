@@ -548,7 +548,8 @@ static int num_sms_of(int dev) {
     return n;
 }
 
-static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int num_sms) {
+static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int num_sms,
+                      const bldm_tuning* tune) {
     const bool aligned = (z * es) % 16 == 0;
     c.vec = aligned ? int(16 / es) : 1;
     const long nch = long((z + c.vec - 1) / c.vec);
@@ -572,22 +573,34 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
     // each stage also owns a [warps][z] slice of S_ipk partials (FP64)
     const size_t per_stage = c.stage_bytes + size_t(kSweepWarps) * z * 8;
     const size_t fixed = 64 + z * es + 128;
-    const size_t budget = 106 * 1024;  // dynamic; + 2 KB static log table per CTA
+    // Shared memory per SM is 228 KB; each CTA also holds 1 KB reserved and
+    // the 2 KB static log table.  Registers (<= 128 per thread) allow at most
+    // two 256-thread CTAs per SM.
+    int cps = (tune && tune->ctas_per_sm > 0) ? tune->ctas_per_sm : 2;
+    if (cps > 2) return BLDM_ERR_UNSUPPORTED;
+    const size_t budget = (cps == 2 ? 110 : 220) * 1024;
     long st = budget > fixed ? long((budget - fixed) / per_stage) : 0;
     st = std::min(8L, st);
+    if (tune && tune->stages > 0) {
+        if (tune->stages > st || tune->stages < 2) return BLDM_ERR_UNSUPPORTED;
+        st = tune->stages;
+    }
     if (st < 2) {
-        // large slabs: allow one CTA per SM
+        if (tune && tune->ctas_per_sm == 2) return BLDM_ERR_UNSUPPORTED;
+        // large slabs: one CTA per SM
+        cps = 1;
         st = std::min(8L, long((220 * 1024 - fixed) / per_stage));
         if (st < 2) return BLDM_ERR_UNSUPPORTED;
     }
     c.stages = int(st);
     c.smem_update = size_t(c.stages) * per_stage + fixed;
     c.smem_sums = c.smem_update;
-    c.ctas_per_sm = c.smem_update + 1024 + 16 * kLogTabN <= 228 * 1024 / 2 ? 2 : 1;
+    c.ctas_per_sm = cps;
     // Row ranges: fill the resident CTA slots in one wave (a partial second
     // wave of a bandwidth-bound sweep costs a whole tail).
     const long target = long(c.ctas_per_sm) * num_sms;
     long nrr = target / c.n_bands;
+    if (tune && tune->row_ranges > 0) nrr = tune->row_ranges;
     nrr = std::max(1L, std::min(long(x), nrr));
     c.n_rr = int(nrr);
     c.rr_base = int(x / nrr);
@@ -602,7 +615,7 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
     return BLDM_OK;
 }
 
-int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype) {
+int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_tuning* tune) {
     if (x == 0 || y == 0 || z == 0) return BLDM_ERR_BAD_ARG;
     if (z > 1024) return BLDM_ERR_UNSUPPORTED;
     if (dtype != BLDM_F64 && dtype != BLDM_F32) return BLDM_ERR_BAD_ARG;
@@ -612,7 +625,7 @@ int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype) {
     p->y = y;
     p->z = z;
     p->esize = dtype == BLDM_F64 ? 8 : 4;
-    int rc = choose_cfg(p->cfg, x, y, z, p->esize, num_sms_of(p->device));
+    int rc = choose_cfg(p->cfg, x, y, z, p->esize, num_sms_of(p->device), tune);
     if (rc) return rc;
     const SweepCfg& c = p->cfg;
     const size_t a = 256;

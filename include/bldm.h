@@ -129,6 +129,21 @@ int bldm_release_cache(void);
 typedef struct bldm_plan bldm_plan;
 
 int bldm_plan_create(bldm_plan** plan, size_t x, size_t y, size_t z, int dtype);
+
+/* Launch knobs of the fused sweep; 0 = chosen by the library.  stages: depth
+ * of the shared-memory ring of bulk-copied row segments (2..8); ctas_per_sm:
+ * resident sweep CTAs per SM (1 or 2); row_ranges: row ranges the rows of a
+ * band of columns are split into (one CTA each).  The reference has no
+ * counterpart (its kernels use fixed 32x32 / 16x16x4 blocks,
+ * cuda_src/bld_mult/bld_mult_cuda_funcs.cu:18-24); the autotuner sets them. */
+typedef struct bldm_tuning {
+    int stages;
+    int ctas_per_sm;
+    int row_ranges;
+} bldm_tuning;
+int bldm_plan_create_tuned(bldm_plan** plan, size_t x, size_t y, size_t z, int dtype,
+                           const bldm_tuning* tuning);
+int bldm_plan_get_tuning(const bldm_plan* plan, bldm_tuning* out);
 int bldm_plan_destroy(bldm_plan* plan);
 /* Bytes of device workspace the plan holds (partials, digamma tables). */
 int bldm_plan_workspace_bytes(const bldm_plan* plan, size_t* bytes);
