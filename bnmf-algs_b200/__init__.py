@@ -24,9 +24,9 @@ LIB_PATH = os.path.join(_HERE, "libbldm.so")
 
 # bldm_status
 OK, ERR_BAD_ARG, ERR_NEG_X, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_NO_DEVICE, \
-    ERR_UNSUPPORTED, ERR_BUSY, ERR_NOT_FOUND = range(10)
+    ERR_UNSUPPORTED, ERR_BUSY, ERR_NOT_FOUND, ERR_TOO_LARGE = range(11)
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "NEG_X", 3: "OOM", 4: "CUDA", 5: "TIMEOUT",
-                6: "NO_DEVICE", 7: "UNSUPPORTED", 8: "BUSY", 9: "NOT_FOUND"}
+                6: "NO_DEVICE", 7: "UNSUPPORTED", 8: "BUSY", 9: "NOT_FOUND", 10: "TOO_LARGE"}
 # bldm_psi_mode
 PSI_EXACT, PSI_APPR, PSI_LEGACY_CUDA = 0, 1, 2
 # bldm_dtype
@@ -117,6 +117,8 @@ SIGNATURES = {
     "bldm_plan_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _sz, ctypes.c_int, ctypes.c_double,
                                      _vp]),
     "bldm_plan_check": (ctypes.c_int, [_vp, _vp]),
+    "bldm_solve_device_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int,
+                                                 _sz, ctypes.c_int, ctypes.c_double, _vp]),
     "bldm_plan_init_S": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp]),
     "bldm_plan_profile": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _sz, ctypes.c_int,
                                          ctypes.c_double, _vp, _dp, _dp]),

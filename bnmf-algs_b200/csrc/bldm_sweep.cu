@@ -675,6 +675,68 @@ int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_
     return BLDM_OK;
 }
 
+// Lays the plan's workspace out in caller-provided device memory `ws` of
+// `ws_cap` bytes instead of allocating it.  Returns BLDM_ERR_TOO_LARGE (and the
+// bytes needed in *ws_needed) when the workspace does not fit.  The counter and
+// error word are cleared on `st`.
+int plan_setup_in(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, void* ws,
+                  size_t ws_cap, size_t* ws_needed, cudaStream_t st) {
+    if (x == 0 || y == 0 || z == 0 || !ws) return BLDM_ERR_BAD_ARG;
+    if (z > 1024) return BLDM_ERR_UNSUPPORTED;
+    if (dtype != BLDM_F64 && dtype != BLDM_F32) return BLDM_ERR_BAD_ARG;
+    BLDM_CU(cudaGetDevice(&p->device));
+    p->dtype = dtype;
+    p->x = x;
+    p->y = y;
+    p->z = z;
+    p->esize = dtype == BLDM_F64 ? 8 : 4;
+    int rc = choose_cfg(p->cfg, x, y, z, p->esize, num_sms_of(p->device), nullptr);
+    if (rc) return rc;
+    const SweepCfg& c = p->cfg;
+    const size_t a = 256;
+    size_t off = 0;
+    const size_t o_pjk = off;
+    off = align_up(off + size_t(c.n_rr) * y * z * 8, a);
+    const size_t o_ipk = off;
+    off = align_up(off + size_t(c.n_bands) * x * z * 8, a);
+    const size_t o_psiB = off;
+    off = align_up(off + y * z * p->esize, a);
+    const size_t o_psiA = off;
+    off = align_up(off + x * z * p->esize, a);
+    const size_t o_psiAS = off;
+    off = align_up(off + z * p->esize, a);
+    const size_t o_asum = off;
+    off = align_up(off + size_t(c.n_ablk) * z * 8, a);
+    const size_t o_cnt = off;
+    off = align_up(off + 64, a);
+    if (ws_needed) *ws_needed = off;
+    if (off > ws_cap) return BLDM_ERR_TOO_LARGE;
+    p->ws = ws;  // not owned: never pass this plan to plan_free
+    p->ws_bytes = off;
+    char* base = static_cast<char*>(ws);
+    p->part_pjk = reinterpret_cast<double*>(base + o_pjk);
+    p->part_ipk = reinterpret_cast<double*>(base + o_ipk);
+    p->psiB = base + o_psiB;
+    p->psiA = base + o_psiA;
+    p->psiAS = base + o_psiAS;
+    p->asum_part = reinterpret_cast<double*>(base + o_asum);
+    p->counter = reinterpret_cast<unsigned*>(base + o_cnt);
+    p->err = reinterpret_cast<int*>(base + o_cnt + 16);
+    BLDM_CU(cudaMemsetAsync(base + o_cnt, 0, 64, st));
+    for (int upd = 0; upd < 2; ++upd)
+        for (int ap = 0; ap < 2; ++ap) {
+            void* fn = nullptr;
+            if (dtype == BLDM_F64)
+                fn = reinterpret_cast<void*>(pick_sweep<double>(c, upd != 0, ap != 0));
+            else
+                fn = reinterpret_cast<void*>(pick_sweep<float>(c, upd != 0, ap != 0));
+            if (!fn) return BLDM_ERR_UNSUPPORTED;
+            BLDM_CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(c.smem_update)));
+        }
+    return BLDM_OK;
+}
+
 void plan_free(PlanImpl* p) {
     if (p->ws) cudaFree(p->ws);
     p->ws = nullptr;

@@ -43,7 +43,8 @@ typedef enum bldm_status {
     BLDM_ERR_NO_DEVICE = 6,   /* no usable CUDA device */
     BLDM_ERR_UNSUPPORTED = 7, /* shape outside the fused kernels' range (z too large) */
     BLDM_ERR_BUSY = 8,        /* serving: no slot or memory for the request now */
-    BLDM_ERR_NOT_FOUND = 9    /* serving: unknown request id */
+    BLDM_ERR_NOT_FOUND = 9,   /* serving: unknown request id */
+    BLDM_ERR_TOO_LARGE = 10   /* the shape's scratch exceeds a fixed scratch area */
 } bldm_status;
 
 /* Digamma selection.
@@ -150,6 +151,25 @@ int bldm_plan_workspace_bytes(const bldm_plan* plan, size_t* bytes);
 int bldm_plan_run(bldm_plan* plan, const void* d_X, const double* d_alpha,
                   const double* d_beta, void* d_S, size_t max_iter,
                   int psi_mode, double eps, void* stream);
+/* The same solve as bldm_plan_run without allocating anything.  No counterpart
+ * in the reference.  For callers that cannot allocate device memory while they
+ * solve: cudaMalloc/cudaFree may synchronise the device (too slow for a
+ * latency-bound serving loop), and a raw allocation can fail with out-of-memory
+ * in a process whose device memory another allocator (a framework's caching
+ * allocator, a server's up-front reservation) already holds.  The solver's
+ * scratch comes from a fixed 32 MiB array in the library's device data, held on
+ * every GPU where the library's device code is loaded until the process exits;
+ * shapes whose scratch exceeds it return BLDM_ERR_TOO_LARGE (1024x1024x64 FP64
+ * needs 22.5 MB).  The caller passes device buffers as for bldm_plan_run (dtype
+ * is BLDM_F64 or BLDM_F32).  The first call on a device looks up the array's
+ * device address on that device (make that first call before any stream
+ * capture).  All calls on a device share the array, and calls that overlap on
+ * the GPU race.  Synchronises `stream` before returning and reports a
+ * device-side error as BLDM_ERR_TIMEOUT. */
+int bldm_solve_device_noalloc(const void* d_X, const double* d_alpha,
+                              const double* d_beta, void* d_S, size_t x, size_t y,
+                              size_t z, int dtype, size_t max_iter, int psi_mode,
+                              double eps, void* stream);
 /* Synchronises `stream` and reports a device-side error recorded by the
  * plan's kernels (BLDM_ERR_TIMEOUT) or a CUDA error. */
 int bldm_plan_check(bldm_plan* plan, void* stream);
