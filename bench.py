@@ -343,6 +343,85 @@ def run_profile(args):
     return 0
 
 
+def run_batch(args):
+    """Batched uneven solves vs looping the plain per-instance solver."""
+    import torch
+    pkg = load_package()
+    import bnmf_algs_b200.workloads as W
+    shapes = W.batch_shapes(args.batch_n, 3)
+    iters = 150
+    f64 = args.dtype == "f64"
+    dtype = pkg.F64 if f64 else pkg.F32
+    es = 8 if f64 else 4
+    upd = sum(x * y * z for x, y, z in shapes) * iters
+    t0 = time.perf_counter()
+    b = pkg.Batch(shapes, dtype=dtype, rows_per_tile=args.rows_per_tile)
+    probs = []
+    for k, (x, y, z) in enumerate(shapes):
+        pr = W.batch_instance((x, y, z), 1000 + 3 * 100003 + k)
+        b.set(k, pr["X"], pr["alpha"], pr["beta"], None, seed=k)
+        probs.append(pr)
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        b.run(iters, pkg.PSI_APPR, 1e-50, True, stream)
+    b.check(stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.info()["launches"]
+    with ClockSampler(0) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.run(iters, pkg.PSI_APPR, 1e-50, True, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    b.check(stream)
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = b.info()["launches"] - l0
+    # loop of the plain per-instance solver (one plan per distinct shape)
+    plans = {}
+    dev = []
+    for (x, y, z), pr in zip(shapes, probs):
+        if (x, y, z) not in plans:
+            plans[(x, y, z)] = pkg.Plan(x, y, z, dtype)
+        tt = torch.float64 if f64 else torch.float32
+        dX = torch.as_tensor(pr["X"]).to("cuda", tt)
+        dS = torch.empty((x, y, z), dtype=tt, device="cuda")
+        plans[(x, y, z)].init_S(dX, dS, seed=0)
+        dev.append((plans[(x, y, z)], dX, torch.as_tensor(pr["alpha"]).cuda(),
+                    torch.as_tensor(pr["beta"]).cuda(), dS))
+    def loop():
+        for plan, dX, da, db, dS in dev:
+            plan.run(dX, da, db, dS, iters, pkg.PSI_APPR, 1e-50, stream)
+    loop()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    loop()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    loop_ms = e0.elapsed_time(e1)
+    alg_bytes = sum(2 * x * y * z * es + x * y * es for x, y, z in shapes) * iters
+    peak, _ = hbm_peak()
+    line = {"metric": "batched_solves_per_s", "value": len(shapes) / (ms / 1e3),
+            "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.dtype, "data": "synthetic",
+            "config": {"workload": f"batch_{len(shapes)}_uneven", "iters": iters,
+                       "x_y": "log-uniform [32,512]", "z": "{4,8,16,32,64}",
+                       "total_S_elements": sum(x * y * z for x, y, z in shapes),
+                       "rows_per_tile": args.rows_per_tile or 64, "graph": True},
+            "S_updates_per_s": upd / (ms / 1e3),
+            "hbm_gbs_algorithmic": alg_bytes / (ms / 1e3) / 1e9,
+            "frac_of_hbm_peak": alg_bytes / (ms / 1e3) / 1e9 / peak,
+            "plain_loop": {"ms": loop_ms, "solves_per_s": len(shapes) / (loop_ms / 1e3),
+                           "S_updates_per_s": upd / (loop_ms / 1e3)},
+            "speedup_vs_plain_loop": loop_ms / ms,
+            "classes": b.info()["classes"], "gpu_launches": launches,
+            "setup_s": setup_s, "clocks": clk.summary()}
+    print(json.dumps(line))
+    b.close()
+    return 0
+
+
 def make_X(kind, x, y, z, rng):
     """X kinds: 'model' (the plain workload's allocation-model draw), 'dense'
     (1 + Poisson(10), no zeros), 'zeros' (all zero)."""
@@ -406,6 +485,11 @@ def main():
     ap.add_argument("--profile-iters", type=int, default=3)
     ap.add_argument("--shape", default="1024x1024x64",
                     help="x*y*z of the plain workload for --profile-run / --kernel-matrix")
+    ap.add_argument("--batch", action="store_true",
+                    help="batched uneven solves: 512 instances, x,y log-uniform in [32,512], "
+                         "z in {4..64}, FP32, 150 iterations; vs a loop of the plain solver")
+    ap.add_argument("--batch-n", type=int, default=512)
+    ap.add_argument("--rows-per-tile", type=int, default=0)
     ap.add_argument("--kernel-matrix", action="store_true",
                     help="time the update sweep (CUDA events) over X kinds, dtypes and launch "
                          "knobs; one JSON line each")
@@ -414,6 +498,8 @@ def main():
         return run_profile(args)
     if args.kernel_matrix:
         return run_kernel_matrix(args)
+    if args.batch:
+        return run_batch(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

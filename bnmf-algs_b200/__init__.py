@@ -135,6 +135,19 @@ SIGNATURES = {
     "bldm_psi_f32": (ctypes.c_int, [_vp, _sz, _vp, _vp]),
     "bldm_log_marginal_S": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _sz, _sz, _dp, _dp,
                                            ctypes.c_double, ctypes.c_double, _dp, _vp]),
+    "bldm_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _sz,
+                                         ctypes.POINTER(_sz), ctypes.POINTER(_sz),
+                                         ctypes.POINTER(_sz), ctypes.c_int]),
+    "bldm_batch_destroy": (ctypes.c_int, [_vp]),
+    "bldm_batch_set": (ctypes.c_int, [_vp, _sz, _dp, _dp, _dp, _dp, ctypes.c_uint64]),
+    "bldm_batch_run": (ctypes.c_int, [_vp, _sz, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                      _vp]),
+    "bldm_batch_check": (ctypes.c_int, [_vp, _vp]),
+    "bldm_batch_get": (ctypes.c_int, [_vp, _sz, _dp, _dp]),
+    "bldm_batch_device_ptrs": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp),
+                                              ctypes.POINTER(_vp)]),
+    "bldm_batch_info": (ctypes.c_int, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz),
+                                       ctypes.POINTER(ctypes.c_uint64)]),
     "bldm_version": (ctypes.c_char_p, []),
 }
 
@@ -378,3 +391,62 @@ def psi(d_in, appr=True, stream=None):
     else:
         _check(lib().bldm_psi_f32(_ptr(d_in), d_in.numel(), _ptr(out), _stream_ptr(stream)))
     return out
+
+
+class Batch:
+    """bldm_batch: independent instances of different shapes solved together."""
+
+    def __init__(self, shapes, dtype=F32, rows_per_tile=0):
+        n = len(shapes)
+        arr = lambda v: (ctypes.c_size_t * n)(*v)
+        self.shapes = [tuple(int(v) for v in s) for s in shapes]
+        self.dtype = dtype
+        self._h = ctypes.c_void_p()
+        _check(lib().bldm_batch_create(ctypes.byref(self._h), dtype, n,
+                                       arr([s[0] for s in self.shapes]),
+                                       arr([s[1] for s in self.shapes]),
+                                       arr([s[2] for s in self.shapes]), int(rows_per_tile)),
+               "batch_create")
+
+    def close(self):
+        if self._h:
+            lib().bldm_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set(self, idx, X, alpha, beta, S0=None, seed=0):
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        alpha = np.ascontiguousarray(alpha, dtype=np.float64)
+        beta = np.ascontiguousarray(beta, dtype=np.float64)
+        S0p = None
+        if S0 is not None:
+            S0 = np.ascontiguousarray(S0, dtype=np.float64)
+            S0p = S0.ctypes.data_as(_dp)
+        _check(lib().bldm_batch_set(self._h, idx, X.ctypes.data_as(_dp),
+                                    alpha.ctypes.data_as(_dp), beta.ctypes.data_as(_dp), S0p,
+                                    int(seed)), "batch_set")
+
+    def run(self, iters, psi_mode=PSI_APPR, eps=1e-50, use_graph=True, stream=None):
+        _check(lib().bldm_batch_run(self._h, int(iters), int(psi_mode), float(eps),
+                                    1 if use_graph else 0, _stream_ptr(stream)), "batch_run")
+
+    def check(self, stream=None):
+        _check(lib().bldm_batch_check(self._h, _stream_ptr(stream)), "batch_check")
+
+    def get(self, idx):
+        x, y, z = self.shapes[idx]
+        S = np.empty((x, y, z))
+        rel = ctypes.c_double()
+        _check(lib().bldm_batch_get(self._h, idx, S.ctypes.data_as(_dp), ctypes.byref(rel)))
+        return S, rel.value
+
+    def info(self):
+        nc, nb, nl = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_uint64()
+        _check(lib().bldm_batch_info(self._h, ctypes.byref(nc), ctypes.byref(nb),
+                                     ctypes.byref(nl)))
+        return {"classes": nc.value, "device_bytes": nb.value, "launches": nl.value}

@@ -1,0 +1,417 @@
+// Multi-instance engine (see bldm_engine.h).
+#include <algorithm>
+#include <cstring>
+
+#include "bldm_engine.h"
+
+namespace bldm {
+
+namespace {
+
+size_t a256(size_t v) { return (v + 255) & ~size_t(255); }
+
+int sms_of_current_device() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+        return 148;
+    return n;
+}
+
+#define ENG_CU(call)                                    \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_status(e_);  \
+    } while (0)
+
+}  // namespace
+
+size_t InstanceBytes::total(size_t align) const {
+    const size_t parts[] = {X, S, alpha, beta, pjk, ipk, psiB, psiA, psiAS, asum, counter, delta,
+                            rel};
+    size_t t = 0;
+    for (size_t p : parts) t += (p + align - 1) / align * align;
+    return t;
+}
+
+Engine::Engine(int dtype, int rows_per_tile)
+    : dtype_(dtype), es_(dtype == BLDM_F64 ? 8 : 4),
+      rows_per_tile_(rows_per_tile > 0 ? rows_per_tile : 64),
+      num_sms_(sms_of_current_device()) {
+    cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming);
+}
+
+Engine::~Engine() {
+    drop_graphs();
+    free_tables();
+    for (auto& c : classes_) {
+        if (c.stream) cudaStreamDestroy(c.stream);
+        if (c.done) cudaEventDestroy(c.done);
+    }
+    if (fork_) cudaEventDestroy(fork_);
+}
+
+int Engine::configure(EngineInstance& in, size_t x, size_t y, size_t z) const {
+    if (x == 0 || y == 0 || z == 0) return BLDM_ERR_BAD_ARG;
+    if (z > 1024) return BLDM_ERR_UNSUPPORTED;
+    in.x = x;
+    in.y = y;
+    in.z = z;
+    SweepCfg& c = in.cfg;
+    if (lane_config(z, es_, c) != BLDM_OK) return BLDM_ERR_UNSUPPORTED;
+    const int fpw = 32 / c.lpf;
+    c.warps = kSweepWarps;
+    c.wpr = kSweepWarps;
+    while (c.wpr > 1 && size_t(c.wpr / 2) * c.cpw * fpw >= y) c.wpr /= 2;
+    c.band_w = c.wpr * c.cpw * fpw;
+    c.n_bands = int((y + c.band_w - 1) / c.band_w);
+    const int rps = kSweepWarps / c.wpr;
+    const int R = std::max(rps, (rows_per_tile_ + rps - 1) / rps * rps);
+    c.n_rr = int((x + R - 1) / R);
+    c.rr_base = R;
+    c.rr_extra = 0;
+    const SlotLayout lay((long long)c.band_w, (long long)z, int(es_));
+    in.stage_need = uint32_t(rps) * (lay.capS + lay.capX + lay.capA);
+    const int KT = int(std::min<size_t>(z, kFinThreads));
+    const int Rf = kFinThreads / KT;
+    const long rows = std::max<long>(Rf, long((x + 127) / 128));
+    c.rows_per_ablk = int(rows);
+    c.n_ablk = int((x + rows - 1) / rows);
+    in.nbB = int((y * z + kFinThreads - 1) / kFinThreads);
+    return BLDM_OK;
+}
+
+InstanceBytes Engine::bytes(const EngineInstance& in) const {
+    const SweepCfg& c = in.cfg;
+    InstanceBytes b;
+    b.X = in.x * in.y * es_;
+    b.S = in.x * in.y * in.z * es_;
+    b.alpha = in.x * 8;
+    b.beta = in.z * 8;
+    b.pjk = size_t(c.n_rr) * in.y * in.z * 8;
+    b.ipk = size_t(c.n_bands) * in.x * in.z * 8;
+    b.psiB = in.y * in.z * es_;
+    b.psiA = in.x * in.z * es_;
+    b.psiAS = in.z * es_;
+    b.asum = size_t(c.n_ablk) * in.z * 8;
+    b.counter = 16;
+    b.delta = size_t(c.n_rr) * c.n_bands * 16;
+    b.rel = 8;
+    return b;
+}
+
+void Engine::bind(EngineInstance& in, void* base) const {
+    const InstanceBytes b = bytes(in);
+    char* p = static_cast<char*>(base);
+    auto take = [&](size_t n) {
+        char* q = p;
+        p += a256(n);
+        return q;
+    };
+    in.X = take(b.X);
+    in.S = take(b.S);
+    in.alpha = reinterpret_cast<double*>(take(b.alpha));
+    in.beta = reinterpret_cast<double*>(take(b.beta));
+    in.part_pjk = reinterpret_cast<double*>(take(b.pjk));
+    in.part_ipk = reinterpret_cast<double*>(take(b.ipk));
+    in.psiB = take(b.psiB);
+    in.psiA = take(b.psiA);
+    in.psiAS = take(b.psiAS);
+    in.asum = reinterpret_cast<double*>(take(b.asum));
+    in.counter = reinterpret_cast<unsigned*>(take(b.counter));
+    in.delta = reinterpret_cast<double*>(take(b.delta));
+    in.rel = reinterpret_cast<double*>(take(b.rel));
+}
+
+void Engine::free_tables() {
+    for (auto& c : classes_) {
+        if (c.d_tiles) cudaFree(c.d_tiles);
+        c.d_tiles = nullptr;
+    }
+    if (d_tables_) cudaFree(d_tables_);
+    d_tables_ = nullptr;
+    table_bytes_ = 0;
+}
+
+void Engine::drop_graphs() {
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.second);
+    graphs_.clear();
+}
+
+template <typename T>
+static void fill_tables(const std::vector<EngineInstance*>& insts, std::vector<char>& host,
+                        size_t o_sinst, size_t o_finst) {
+    SweepInst<T>* si = reinterpret_cast<SweepInst<T>*>(host.data() + o_sinst);
+    FinInst<T>* fi = reinterpret_cast<FinInst<T>*>(host.data() + o_finst);
+    for (size_t n = 0; n < insts.size(); ++n) {
+        const EngineInstance& in = *insts[n];
+        const SweepCfg& c = in.cfg;
+        SweepInst<T>& s = si[n];
+        s.S = static_cast<T*>(in.S);
+        s.X = static_cast<const T*>(in.X);
+        s.psiB = static_cast<const T*>(in.psiB);
+        s.psiA = static_cast<const T*>(in.psiA);
+        s.psiAS = static_cast<const T*>(in.psiAS);
+        s.part_pjk = in.part_pjk;
+        s.part_ipk = in.part_ipk;
+        s.delta_part = in.delta;
+        s.x = (long long)in.x;
+        s.y = (long long)in.y;
+        s.z = (long long)in.z;
+        s.n_bands = c.n_bands;
+        s.band_w = c.band_w;
+        s.wpr = c.wpr;
+        s.n_rr = c.n_rr;
+        s.rr_base = c.rr_base;
+        s.rr_extra = c.rr_extra;
+        FinInst<T>& f = fi[n];
+        f.part_pjk = in.part_pjk;
+        f.part_ipk = in.part_ipk;
+        f.alpha = in.alpha;
+        f.beta = in.beta;
+        f.psiB = static_cast<T*>(in.psiB);
+        f.psiA = static_cast<T*>(in.psiA);
+        f.psiAS = static_cast<T*>(in.psiAS);
+        f.asum_part = in.asum;
+        f.counter = in.counter;
+        f.delta_part = in.delta;
+        f.rel_change = in.rel;
+        f.x = (long long)in.x;
+        f.y = (long long)in.y;
+        f.z = (long long)in.z;
+        f.n_rr = c.n_rr;
+        f.n_bands = c.n_bands;
+        f.nbB = in.nbB;
+        f.n_ablk = c.n_ablk;
+        f.rows_per_ablk = c.rows_per_ablk;
+        f.n_tiles = c.n_rr * c.n_bands;
+    }
+}
+
+int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
+    drop_graphs();
+    free_tables();
+    insts_ = insts;
+    // Lane-shape classes, keeping streams of classes that already exist.
+    std::vector<ShapeClass> old;
+    old.swap(classes_);
+    auto class_of = [&](const SweepCfg& c) -> ShapeClass& {
+        for (auto& k : classes_)
+            if (k.vec == c.vec && k.lpf == c.lpf && k.mch == c.mch) return k;
+        ShapeClass k;
+        k.vec = c.vec;
+        k.lpf = c.lpf;
+        k.mch = c.mch;
+        classes_.push_back(k);
+        return classes_.back();
+    };
+    for (EngineInstance* in : insts) {
+        ShapeClass& k = class_of(in->cfg);
+        k.max_z = std::max(k.max_z, in->z);
+        k.stage_bytes = std::max(k.stage_bytes, in->stage_need);
+    }
+    for (size_t i = 0; i < classes_.size(); ++i) {
+        if (i < old.size()) {
+            classes_[i].stream = old[i].stream;
+            classes_[i].done = old[i].done;
+            old[i].stream = nullptr;
+            old[i].done = nullptr;
+        } else {
+            ENG_CU(cudaStreamCreateWithFlags(&classes_[i].stream, cudaStreamNonBlocking));
+            ENG_CU(cudaEventCreateWithFlags(&classes_[i].done, cudaEventDisableTiming));
+        }
+    }
+    for (auto& k : old) {
+        if (k.stream) cudaStreamDestroy(k.stream);
+        if (k.done) cudaEventDestroy(k.done);
+    }
+    // Ring depth and shared memory per class (2 CTAs/SM when they fit).
+    for (auto& k : classes_) {
+        const size_t per_stage = k.stage_bytes + size_t(kSweepWarps) * k.max_z * 8;
+        const size_t fixed = 64 + k.max_z * es_ + 128;
+        long s = long((110 * 1024 - std::min<size_t>(fixed, 110 * 1024)) / per_stage);
+        if (s < 2) s = long((220 * 1024 - std::min<size_t>(fixed, 220 * 1024)) / per_stage);
+        if (s < 2) return BLDM_ERR_UNSUPPORTED;
+        k.stages = int(std::min(8L, s));
+        k.smem = size_t(k.stages) * per_stage + fixed;
+        for (int upd = 0; upd < 2; ++upd)
+            for (int ap = 0; ap < 2; ++ap) {
+                void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, upd != 0, ap != 0, true);
+                if (!fn) return BLDM_ERR_UNSUPPORTED;
+                ENG_CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(k.smem)));
+            }
+    }
+    // Tiles of every instance, per class.
+    for (size_t n = 0; n < insts.size(); ++n) {
+        const EngineInstance& in = *insts[n];
+        const SweepCfg& c = in.cfg;
+        ShapeClass& k = class_of(c);
+        const int rps = kSweepWarps / c.wpr;
+        if (rps > 1 &&
+            size_t(rps) * c.band_w * in.z * 8 > size_t(k.stages) * size_t(k.stage_bytes))
+            return BLDM_ERR_UNSUPPORTED;
+        for (int rr = 0; rr < c.n_rr; ++rr)
+            for (int b = 0; b < c.n_bands; ++b) k.tiles.push_back(BatchTile{int(n), b, rr, 0});
+    }
+    // Device tables: SweepInst[n] | FinInst[n] | block_off[n+1] | err.
+    const size_t n = insts.size();
+    const size_t s_sz = dtype_ == BLDM_F64 ? sizeof(SweepInst<double>) : sizeof(SweepInst<float>);
+    const size_t f_sz = dtype_ == BLDM_F64 ? sizeof(FinInst<double>) : sizeof(FinInst<float>);
+    const size_t o_sinst = 0;
+    const size_t o_finst = a256(o_sinst + n * s_sz);
+    const size_t o_boff = a256(o_finst + n * f_sz);
+    const size_t o_err = a256(o_boff + (n + 1) * sizeof(int));
+    table_bytes_ = a256(o_err + 64);
+    std::vector<char> host(table_bytes_, 0);
+    if (dtype_ == BLDM_F64)
+        fill_tables<double>(insts, host, o_sinst, o_finst);
+    else
+        fill_tables<float>(insts, host, o_sinst, o_finst);
+    int* boff = reinterpret_cast<int*>(host.data() + o_boff);
+    fin_blocks_ = 0;
+    for (size_t i = 0; i < n; ++i) {
+        boff[i] = fin_blocks_;
+        fin_blocks_ += insts[i]->nbB + insts[i]->cfg.n_ablk;
+    }
+    boff[n] = fin_blocks_;
+    ENG_CU(cudaMalloc(&d_tables_, table_bytes_));
+    char* base = static_cast<char*>(d_tables_);
+    d_sinst_ = base + o_sinst;
+    d_finst_ = base + o_finst;
+    d_block_off_ = reinterpret_cast<int*>(base + o_boff);
+    d_err_ = reinterpret_cast<int*>(base + o_err);
+    ENG_CU(cudaMemcpy(d_tables_, host.data(), table_bytes_, cudaMemcpyHostToDevice));
+    for (auto& k : classes_) {
+        ENG_CU(cudaMalloc(&k.d_tiles, k.tiles.size() * sizeof(BatchTile)));
+        ENG_CU(cudaMemcpy(k.d_tiles, k.tiles.data(), k.tiles.size() * sizeof(BatchTile),
+                          cudaMemcpyHostToDevice));
+        table_bytes_ += k.tiles.size() * sizeof(BatchTile);
+    }
+    for (EngineInstance* in : insts) ENG_CU(cudaMemsetAsync(in->counter, 0, 16, st));
+    return BLDM_OK;
+}
+
+template <typename T>
+static void launch_class_kernel(void* fn, unsigned grid, size_t smem, cudaStream_t s,
+                                const void* d_sinst, const BatchTile* d_tiles, int stages,
+                                uint32_t stage_bytes, double eps, int* err, bool track) {
+    BatchSweepParams<T> p;
+    p.insts = static_cast<const SweepInst<T>*>(d_sinst);
+    p.tiles = d_tiles;
+    p.L.stages = stages;
+    p.L.stage_bytes = stage_bytes;
+    p.L.eps = eps;
+    p.L.err = err;
+    p.track = track ? 1 : 0;
+    reinterpret_cast<void (*)(const BatchSweepParams<T>)>(fn)<<<grid, kSweepThreads, smem, s>>>(p);
+}
+
+int Engine::launch_sweeps(bool update, bool appr, bool track, double eps, cudaStream_t st) {
+    const bool fork = classes_.size() > 1;
+    if (fork) ENG_CU(cudaEventRecord(fork_, st));
+    for (auto& k : classes_) {
+        if (k.tiles.empty()) continue;
+        cudaStream_t s = fork ? k.stream : st;
+        if (fork) ENG_CU(cudaStreamWaitEvent(s, fork_, 0));
+        void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, update, appr, true);
+        if (dtype_ == BLDM_F64)
+            launch_class_kernel<double>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_,
+                                        k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track);
+        else
+            launch_class_kernel<float>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_,
+                                       k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track);
+        ENG_CU(cudaGetLastError());
+        launches_ += 1;
+        if (fork) ENG_CU(cudaEventRecord(k.done, s));
+    }
+    if (fork)
+        for (auto& k : classes_)
+            if (!k.tiles.empty()) ENG_CU(cudaStreamWaitEvent(st, k.done, 0));
+    return BLDM_OK;
+}
+
+template <typename T>
+static void launch_fin_kernel(unsigned grid, cudaStream_t s, const void* d_finst,
+                              const int* d_boff, int n, int plus_appr, int minus_appr) {
+    BatchFinParams<T> p;
+    p.insts = static_cast<const FinInst<T>*>(d_finst);
+    p.block_off = d_boff;
+    p.n_inst = n;
+    p.plus_appr = plus_appr;
+    p.minus_appr = minus_appr;
+    void* fn = finalize_batch_fn(sizeof(T) == 8 ? BLDM_F64 : BLDM_F32);
+    reinterpret_cast<void (*)(const BatchFinParams<T>)>(fn)<<<grid, kFinThreads, 0, s>>>(p);
+}
+
+int Engine::launch_finalize(int plus_appr, int minus_appr, cudaStream_t st) {
+    if (dtype_ == BLDM_F64)
+        launch_fin_kernel<double>(unsigned(fin_blocks_), st, d_finst_, d_block_off_,
+                                  int(insts_.size()), plus_appr, minus_appr);
+    else
+        launch_fin_kernel<float>(unsigned(fin_blocks_), st, d_finst_, d_block_off_,
+                                 int(insts_.size()), plus_appr, minus_appr);
+    launches_ += 1;
+    return cuda_status(cudaGetLastError());
+}
+
+int Engine::launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st) {
+    const int plus_appr = psi_mode != BLDM_PSI_EXACT;
+    const int minus_appr = psi_mode == BLDM_PSI_APPR;
+    int rc = launch_sweeps(false, true, false, eps, st);
+    if (rc) return rc;
+    rc = launch_finalize(plus_appr, minus_appr, st);
+    if (rc) return rc;
+    for (size_t it = 0; it < iters; ++it) {
+        rc = launch_sweeps(true, plus_appr != 0, it + 1 == iters, eps, st);
+        if (rc) return rc;
+        rc = launch_finalize(plus_appr, minus_appr, st);
+        if (rc) return rc;
+    }
+    return BLDM_OK;
+}
+
+int Engine::run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStream_t st) {
+    if (psi_mode < BLDM_PSI_EXACT || psi_mode > BLDM_PSI_LEGACY_CUDA) return BLDM_ERR_BAD_ARG;
+    if (iters == 0 || insts_.empty()) return BLDM_OK;
+    if (!use_graph || st == nullptr) return launch_sequence(iters, psi_mode, eps, st);
+    uint64_t eb;
+    std::memcpy(&eb, &eps, sizeof eb);
+    const auto key = std::make_tuple(iters, psi_mode, eb);
+    auto it = graphs_.find(key);
+    if (it == graphs_.end()) {
+        const uint64_t l0 = launches_;
+        ENG_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int rc = launch_sequence(iters, psi_mode, eps, st);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(st, &g);
+        launches_ = l0;
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        ENG_CU(ce);
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        ENG_CU(ie);
+        it = graphs_.emplace(key, exec).first;
+    }
+    ENG_CU(cudaGraphLaunch(it->second, st));
+    launches_ += (iters + 1) * (classes_.size() + 1);
+    return BLDM_OK;
+}
+
+int Engine::check(cudaStream_t st) {
+    ENG_CU(cudaStreamSynchronize(st));
+    if (!d_err_) return BLDM_OK;
+    int herr = 0;
+    ENG_CU(cudaMemcpy(&herr, d_err_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) {
+        ENG_CU(cudaMemset(d_err_, 0, sizeof(int)));
+        return BLDM_ERR_TIMEOUT;
+    }
+    return BLDM_OK;
+}
+
+}  // namespace bldm

@@ -1,0 +1,115 @@
+// Multi-instance engine: runs the fused sweep and finalize over many
+// independent BLD instances of different shapes at once.  Used by the batched
+// solver (bldm_batch_*) and the serving loop (bldm_server_*).
+//
+// An iteration of every instance is one sweep launch per lane-shape class
+// (instances whose z maps to the same kernel), the classes running
+// concurrently on forked streams, then one finalize launch for all instances.
+// Tiles (band x row range) of every instance of a class form the class grid;
+// the tiling of an instance depends only on its own shape, so its results do
+// not depend on which other instances share the launches.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "bldm_internal.h"
+#include "bldm_kernels.h"
+
+namespace bldm {
+
+// One instance: shape, derived geometry and device buffers.
+struct EngineInstance {
+    size_t x = 0, y = 0, z = 0;
+    SweepCfg cfg{};      // lane shape, wpr, band_w, n_bands, n_rr, rr_base, n_ablk...
+    int nbB = 0;         // finalize blocks for psi(beta_eph)
+    uint32_t stage_need = 0;
+    // device buffers (owned by the engine's user)
+    void* X = nullptr;
+    void* S = nullptr;
+    double* alpha = nullptr;
+    double* beta = nullptr;
+    double* part_pjk = nullptr;
+    double* part_ipk = nullptr;
+    void* psiB = nullptr;
+    void* psiA = nullptr;
+    void* psiAS = nullptr;
+    double* asum = nullptr;
+    unsigned* counter = nullptr;
+    double* delta = nullptr;
+    double* rel = nullptr;
+};
+
+// Byte sizes of an instance's buffers, in the order of EngineInstance's fields.
+struct InstanceBytes {
+    size_t X, S, alpha, beta, pjk, ipk, psiB, psiA, psiAS, asum, counter, delta, rel;
+    size_t total(size_t align) const;
+};
+
+class Engine {
+  public:
+    Engine(int dtype, int rows_per_tile);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // Geometry of an instance of this shape (no device work).
+    int configure(EngineInstance& in, size_t x, size_t y, size_t z) const;
+    InstanceBytes bytes(const EngineInstance& in) const;
+    // Points the instance's buffers into `base` (InstanceBytes layout, 256-aligned).
+    void bind(EngineInstance& in, void* base) const;
+
+    // (Re)builds the launch tables for the given instances; the pointers must
+    // stay valid until the next build.  Clears the per-instance counters on st.
+    int build(const std::vector<EngineInstance*>& insts, cudaStream_t st);
+    // Runs `iters` iterations of every instance (from the S currently in the
+    // buffers), tracking the relative change of the last one.
+    int run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStream_t st);
+    int check(cudaStream_t st);
+
+    int dtype() const { return dtype_; }
+    size_t es() const { return es_; }
+    size_t n_classes() const { return classes_.size(); }
+    uint64_t launches() const { return launches_; }
+    size_t table_bytes() const { return table_bytes_; }
+
+  private:
+    struct ShapeClass {
+        int vec, lpf, mch;
+        size_t max_z = 0;
+        uint32_t stage_bytes = 0;
+        int stages = 0;
+        size_t smem = 0;
+        std::vector<BatchTile> tiles;
+        BatchTile* d_tiles = nullptr;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;
+    };
+    int launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st);
+    int launch_sweeps(bool update, bool appr, bool track, double eps, cudaStream_t st);
+    int launch_finalize(int plus_appr, int minus_appr, cudaStream_t st);
+    void free_tables();
+    void drop_graphs();
+
+    int dtype_;
+    size_t es_;
+    int rows_per_tile_;
+    int num_sms_;
+    std::vector<EngineInstance*> insts_;
+    std::vector<ShapeClass> classes_;
+    void* d_tables_ = nullptr;  // SweepInst[n] | FinInst[n] | block_off[n+1] | err
+    size_t table_bytes_ = 0;
+    void* d_sinst_ = nullptr;
+    void* d_finst_ = nullptr;
+    int* d_block_off_ = nullptr;
+    int* d_err_ = nullptr;
+    int fin_blocks_ = 0;
+    cudaEvent_t fork_ = nullptr;
+    uint64_t launches_ = 0;
+    std::map<std::tuple<size_t, int, uint64_t>, cudaGraphExec_t> graphs_;
+};
+
+}  // namespace bldm

@@ -22,13 +22,13 @@ struct SweepCfg {
     int mch;        // chunks (of vec elements) per lane
     int cpw;        // fiber passes per warp per row
     int warps;      // warps per CTA
+    int wpr;        // warps per row (8 / wpr rows share a stage)
     int band_w;     // columns per band
     int n_bands;
     int n_rr;       // row ranges
     int rr_base, rr_extra;
     int stages;     // bulk-copy pipeline depth
     int ctas_per_sm;  // resident sweep CTAs per SM (shared-memory bound)
-    uint32_t capS, capX, capA;  // bytes per stage of each slab
     uint32_t stage_bytes;
     size_t smem_update, smem_sums;
     int n_ablk, rows_per_ablk;  // finalize: row blocks for alpha_eph
@@ -66,5 +66,6 @@ int plan_init_S(PlanImpl* p, const void* dX, void* dS, uint64_t seed, cudaStream
 int plan_check(PlanImpl* p, cudaStream_t st);
 
 int cuda_status(cudaError_t e);
+int lane_config(size_t z, size_t es, SweepCfg& c);
 
 }  // namespace bldm

@@ -1,0 +1,109 @@
+// Parameter blocks of the sweep and finalize kernels, shared by the
+// single-instance plan (bldm_sweep.cu) and the multi-instance engine
+// (bldm_batch.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bldm {
+
+constexpr int kSweepWarps = 8;
+constexpr int kSweepThreads = kSweepWarps * 32;
+constexpr int kFinThreads = 256;
+
+// fiber passes per warp per row, from the bytes a lane holds per fiber
+__host__ __device__ constexpr int cpw_for(int bytes) { return bytes <= 16 ? 4 : (bytes <= 32 ? 2 : 1); }
+
+// One instance as a sweep sees it.  Rows are split into row ranges of
+// rr_base (+1 for the first rr_extra ranges) rows, clamped to x; columns into
+// bands of band_w = wpr * CPW * (32 / LPF) columns; wpr warps share one row,
+// so a stage holds 8 / wpr rows.
+template <typename T> struct SweepInst {
+    T* S;
+    const T* X;
+    const T* psiB;       // psi(beta_eph) [y][z]
+    const T* psiA;       // psi(alpha_eph) [x][z]
+    const T* psiAS;      // psi(sum_i alpha_eph) [z]
+    double* part_pjk;    // [n_rr][y][z]
+    double* part_ipk;    // [n_bands][x][z]
+    double* delta_part;  // [n_rr * n_bands][2] (sum |S_new - S|, sum |S_new|) or null
+    long long x, y, z;
+    int n_bands, band_w, wpr;
+    int n_rr, rr_base, rr_extra;
+};
+
+// Launch-wide constants: ring depth, bytes per stage, eps, error word.
+struct SweepLaunch {
+    int stages;
+    uint32_t stage_bytes;
+    double eps;
+    int* err;
+};
+
+template <typename T> struct SweepParams {
+    SweepInst<T> in;
+    SweepLaunch L;
+};
+
+// Multi-instance launch: CTA b works on tile tiles[b] of instance insts[.].
+struct BatchTile {
+    int inst, band, rr, pad;
+};
+template <typename T> struct BatchSweepParams {
+    const SweepInst<T>* insts;
+    const BatchTile* tiles;
+    SweepLaunch L;
+    int track;  // accumulate the relative-change partials in this sweep
+};
+
+// Stage layout for an instance: RPS = 8 / wpr row slots, each with the S
+// segment of the band, the X segment and (UPDATE) the psi(alpha_eph) row, each
+// copied as its enclosing 16-byte-aligned byte range.
+struct SlotLayout {
+    uint32_t capS, capX, capA;
+    __host__ __device__ static uint32_t a16(unsigned long long v) {
+        return uint32_t((v + 15) & ~15ull);
+    }
+    __host__ __device__ SlotLayout(long long band_w, long long z, int es)
+        : capS(a16((unsigned long long)(band_w * z * es + 32))),
+          capX(a16((unsigned long long)(band_w * es + 32))),
+          capA(a16((unsigned long long)(z * es + 32))) {}
+};
+
+// One instance as the finalize step sees it.
+template <typename T> struct FinInst {
+    const double* part_pjk;
+    const double* part_ipk;
+    const double* alpha;
+    const double* beta;
+    T* psiB;
+    T* psiA;
+    T* psiAS;
+    double* asum_part;
+    unsigned* counter;
+    const double* delta_part;  // [n_tiles][2] or null
+    double* rel_change;        // sum |S_new - S| / sum |S_new| of the last sweep
+    long long x, y, z;
+    int n_rr, n_bands, nbB, n_ablk, rows_per_ablk, n_tiles;
+};
+
+template <typename T> struct FinParams {
+    FinInst<T> f;
+    int plus_appr, minus_appr;
+};
+
+template <typename T> struct BatchFinParams {
+    const FinInst<T>* insts;
+    const int* block_off;  // [n_inst + 1] first block of each instance
+    int n_inst;
+    int plus_appr, minus_appr;
+};
+
+// Kernel entry points by lane shape (defined in bldm_sweep.cu).
+void* pick_sweep_fn(int dtype, int vec, int lpf, int mch, bool update, bool appr, bool batch);
+void* finalize_batch_fn(int dtype);
+int launch_init_S(int dtype, const void* dX, void* dS, long long nf, long long z, uint64_t seed,
+                  cudaStream_t st);
+
+}  // namespace bldm

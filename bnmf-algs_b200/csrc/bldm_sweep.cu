@@ -25,30 +25,9 @@
 
 #include "bldm_device.cuh"
 #include "bldm_internal.h"
+#include "bldm_kernels.h"
 
 namespace bldm {
-
-constexpr int kSweepWarps = 8;
-constexpr int kSweepThreads = kSweepWarps * 32;
-constexpr int kFinThreads = 256;
-
-// fiber passes per warp per row, from the bytes a lane holds per fiber
-__host__ __device__ constexpr int cpw_for(int bytes) { return bytes <= 16 ? 4 : (bytes <= 32 ? 2 : 1); }
-
-template <typename T> struct SweepParams {
-    T* S;
-    const T* X;
-    const T* psiB;   // psi(beta_eph) [y][z]
-    const T* psiA;   // psi(alpha_eph) [x][z]
-    const T* psiAS;  // psi(sum_i alpha_eph) [z]
-    double* part_pjk;
-    double* part_ipk;
-    int* err;
-    long long x, y, z;
-    int n_bands, band_w, rr_base, rr_extra, stages;
-    uint32_t capS, capX, stage_bytes;
-    double eps;
-};
 
 template <typename T, int VEC> struct VecIO {
     __device__ __forceinline__ static void load(const T* p, T (&v)[VEC]) {
@@ -88,43 +67,50 @@ __device__ __forceinline__ uintptr_t align_up16(uintptr_t a) {
     return (a + 15) & ~uintptr_t(15);
 }
 
-// Block layout: blockIdx.x = rr * n_bands + band.  Lane layout: lane = g*LPF+q
-// handles fiber slot g of the warp and elements k = (m*LPF + q)*VEC + v.
+// The sweep over one tile (band, row range) of one instance.  Lane layout:
+// lane = g*LPF + q handles fiber slot g of its warp and elements
+// k = (m*LPF + q)*VEC + v; warp w works on row slot w / wpr and column group
+// w % wpr of the band.
 template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR>
-__global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepParams<T> p) {
+__device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLaunch& L, int band,
+                                           int rr, int tile, unsigned char* smem) {
     constexpr int NW = kSweepWarps;
     constexpr int FPW = 32 / LPF;
     constexpr int CPW = cpw_for(MCH * VEC * int(sizeof(T)));
-    extern __shared__ __align__(128) unsigned char smem[];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const int g = lane / LPF;
     const int q = lane % LPF;
+    const int wpr = in.wpr;
+    const int RPS = NW / wpr;
+    const int rs = warp / wpr;  // row slot of this warp
+    const int cg = warp % wpr;  // column group of this warp
 
-    const int band = blockIdx.x % p.n_bands;
-    const int rr = blockIdx.x / p.n_bands;
-    const long long z = p.z;
-    const long long c0 = (long long)band * p.band_w;
-    const int cw = (int)min((long long)p.band_w, p.y - c0);
-    const long long r0 = (long long)rr * p.rr_base + min(rr, p.rr_extra);
-    const int nrows = p.rr_base + (rr < p.rr_extra ? 1 : 0);
+    const long long z = in.z;
+    const long long c0 = (long long)band * in.band_w;
+    const int cw = (int)min((long long)in.band_w, in.y - c0);
+    const long long r0 = (long long)rr * in.rr_base + min(rr, in.rr_extra);
+    const int nrows = (int)min((long long)(in.rr_base + (rr < in.rr_extra ? 1 : 0)), in.x - r0);
+    const int nrounds = (nrows + RPS - 1) / RPS;
+    const SlotLayout lay(in.band_w, z, int(sizeof(T)));
 
     unsigned char* stage0 = smem;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)p.stages * p.stage_bytes);
-    double* red = reinterpret_cast<double*>(bars + 8);         // [stages][NW][z]
-    T* sAS = reinterpret_cast<T*>(red + (size_t)p.stages * NW * z);  // [z]
-    __shared__ int cnt[8];  // per-stage arrivals of warps (monotonic)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)L.stages * L.stage_bytes);
+    double* red = reinterpret_cast<double*>(bars + 8);                    // [stages][NW][z]
+    T* sAS = reinterpret_cast<T*>(red + (size_t)L.stages * NW * z);         // [z]
+    __shared__ int cnt[8];             // per-stage arrivals of warps (monotonic)
+    __shared__ double2 ltab[kLogTabN];  // ln table of the FP64 digamma
+    __shared__ double dsum[NW][2];
 
     if (tid == 0) {
-        for (int s = 0; s < p.stages; ++s) mbar_init(&bars[s], 1);
+        for (int s = 0; s < L.stages; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
     if (tid < 8) cnt[tid] = 0;
-    __shared__ double2 ltab[kLogTabN];  // ln table of the FP64 digamma
     if (UPDATE) {
-        for (long long k = tid; k < z; k += kSweepThreads) sAS[k] = p.psiAS[k];
+        for (long long k = tid; k < z; k += kSweepThreads) sAS[k] = in.psiAS[k];
         if (sizeof(T) == 8 && APPR) log_tab_init(ltab, tid, kSweepThreads);
     }
     __syncthreads();
@@ -132,39 +118,53 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
     const uint64_t pol_stream = policy_evict_first();
     const uint64_t pol_keep = policy_evict_last();
 
-    // Stage t holds row r0+t: the S segment of the band, the X segment and
-    // (UPDATE) the psi(alpha_eph) row, each copied as its enclosing
-    // 16-byte-aligned byte range.
+    auto slotS = [&](unsigned char* st, int r) { return st + (size_t)r * lay.capS; };
+    auto slotX = [&](unsigned char* st, int r) {
+        return st + (size_t)RPS * lay.capS + (size_t)r * lay.capX;
+    };
+    auto slotA = [&](unsigned char* st, int r) {
+        return st + (size_t)RPS * (lay.capS + lay.capX) + (size_t)r * lay.capA;
+    };
+
+    // Round t holds rows r0 + t*RPS + r, r < RPS.
     auto issue = [&](int t) {
-        const long long i = r0 + t;
-        const int s = t % p.stages;
-        unsigned char* st = stage0 + (size_t)s * p.stage_bytes;
-        const uintptr_t aS = reinterpret_cast<uintptr_t>(p.S + (i * p.y + c0) * z);
-        const uintptr_t loS = align_down16(aS);
-        const uintptr_t hiS = align_up16(aS + (uintptr_t)cw * z * sizeof(T));
-        const uintptr_t aX = reinterpret_cast<uintptr_t>(p.X + i * p.y + c0);
-        const uintptr_t loX = align_down16(aX);
-        const uintptr_t hiX = align_up16(aX + (uintptr_t)cw * sizeof(T));
-        uint32_t tot = uint32_t(hiS - loS) + uint32_t(hiX - loX);
-        uintptr_t loA = 0, hiA = 0;
-        if (UPDATE) {
-            const uintptr_t aA = reinterpret_cast<uintptr_t>(p.psiA + i * z);
-            loA = align_down16(aA);
-            hiA = align_up16(aA + (uintptr_t)z * sizeof(T));
-            tot += uint32_t(hiA - loA);
+        const int s = t % L.stages;
+        unsigned char* st = stage0 + (size_t)s * L.stage_bytes;
+        const int nr = min(RPS, nrows - t * RPS);
+        uint32_t tot = 0;
+        for (int r = 0; r < nr; ++r) {
+            const long long i = r0 + (long long)t * RPS + r;
+            const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
+            const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
+            tot += uint32_t(align_up16(aS + (uintptr_t)cw * z * sizeof(T)) - align_down16(aS));
+            tot += uint32_t(align_up16(aX + (uintptr_t)cw * sizeof(T)) - align_down16(aX));
+            if (UPDATE) {
+                const uintptr_t aA = reinterpret_cast<uintptr_t>(in.psiA + i * z);
+                tot += uint32_t(align_up16(aA + (uintptr_t)z * sizeof(T)) - align_down16(aA));
+            }
         }
         mbar_arrive_expect_tx(&bars[s], tot);
-        bulk_g2s(st, reinterpret_cast<const void*>(loS), uint32_t(hiS - loS), &bars[s],
-                 pol_stream);
-        bulk_g2s(st + p.capS, reinterpret_cast<const void*>(loX), uint32_t(hiX - loX), &bars[s],
-                 pol_keep);
-        if (UPDATE)
-            bulk_g2s(st + p.capS + p.capX, reinterpret_cast<const void*>(loA),
-                     uint32_t(hiA - loA), &bars[s], pol_keep);
+        for (int r = 0; r < nr; ++r) {
+            const long long i = r0 + (long long)t * RPS + r;
+            const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
+            const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
+            bulk_g2s(slotS(st, r), reinterpret_cast<const void*>(align_down16(aS)),
+                     uint32_t(align_up16(aS + (uintptr_t)cw * z * sizeof(T)) - align_down16(aS)),
+                     &bars[s], pol_stream);
+            bulk_g2s(slotX(st, r), reinterpret_cast<const void*>(align_down16(aX)),
+                     uint32_t(align_up16(aX + (uintptr_t)cw * sizeof(T)) - align_down16(aX)),
+                     &bars[s], pol_keep);
+            if (UPDATE) {
+                const uintptr_t aA = reinterpret_cast<uintptr_t>(in.psiA + i * z);
+                bulk_g2s(slotA(st, r), reinterpret_cast<const void*>(align_down16(aA)),
+                         uint32_t(align_up16(aA + (uintptr_t)z * sizeof(T)) - align_down16(aA)),
+                         &bars[s], pol_keep);
+            }
+        }
     };
 
     if (tid == 0) {
-        const int n0 = min(p.stages, nrows);
+        const int n0 = min(L.stages, nrounds);
         for (int t = 0; t < n0; ++t) issue(t);
     }
 
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
     Acc<T> pj[CPW][MCH][VEC];
 #pragma unroll
     for (int c = 0; c < CPW; ++c) {
-        const int jl = (warp * CPW + c) * FPW + g;
+        const int jl = (cg * CPW + c) * FPW + g;
 #pragma unroll
         for (int m = 0; m < MCH; ++m) {
 #pragma unroll
@@ -181,46 +181,32 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
                 const long long k = (long long)(m * LPF + q) * VEC + v;
                 pj[c][m][v].init();
                 if (UPDATE)
-                    pB[c][m][v] = (jl < cw && k < z) ? p.psiB[(c0 + jl) * z + k] : T(0);
+                    pB[c][m][v] = (jl < cw && k < z) ? in.psiB[(c0 + jl) * z + k] : T(0);
             }
         }
     }
+    const bool track = UPDATE && in.delta_part != nullptr;
+    double d_abs = 0.0, d_new = 0.0;
 
-    for (int t = 0; t < nrows; ++t) {
-        const int s = t % p.stages;
+    for (int t = 0; t < nrounds; ++t) {
+        const int s = t % L.stages;
         // warp-uniform: the lane-group shuffles below need every lane of the warp
         const bool ok =
-            __all_sync(0xffffffffu, mbar_wait_bounded(&bars[s], (uint32_t)((t / p.stages) & 1)));
+            __all_sync(0xffffffffu, mbar_wait_bounded(&bars[s], (uint32_t)((t / L.stages) & 1)));
         if (!ok) {
             // Give up: flag the error and wait (bounded) for the copies that
             // may still be landing in this CTA's shared memory.
             if (lane == 0) {
-                atomicOr(p.err, DEV_ERR_WAIT_TIMEOUT);
-                const int issued = min(nrows, t + p.stages);
+                atomicOr(L.err, DEV_ERR_WAIT_TIMEOUT);
+                const int issued = min(nrounds, t + L.stages);
                 for (int u = t; u < issued; ++u)
-                    (void)mbar_wait_bounded(&bars[u % p.stages], (uint32_t)((u / p.stages) & 1));
+                    (void)mbar_wait_bounded(&bars[u % L.stages], (uint32_t)((u / L.stages) & 1));
             }
             return;
         }
-        const long long i = r0 + t;
-        const unsigned char* st = stage0 + (size_t)s * p.stage_bytes;
-        const uintptr_t aS = reinterpret_cast<uintptr_t>(p.S + (i * p.y + c0) * z);
-        const uintptr_t aX = reinterpret_cast<uintptr_t>(p.X + i * p.y + c0);
-        const T* sS = reinterpret_cast<const T*>(st + (aS & 15));
-        const T* sX = reinterpret_cast<const T*>(st + p.capS + (aX & 15));
-
-        T gm[MCH][VEC];
-        if (UPDATE) {
-            const uintptr_t aA = reinterpret_cast<uintptr_t>(p.psiA + i * z);
-            const T* sA = reinterpret_cast<const T*>(st + p.capS + p.capX + (aA & 15));
-#pragma unroll
-            for (int m = 0; m < MCH; ++m)
-#pragma unroll
-                for (int v = 0; v < VEC; ++v) {
-                    const long long k = (long long)(m * LPF + q) * VEC + v;
-                    gm[m][v] = (k < z) ? sAS[k] - sA[k] : T(0);
-                }
-        }
+        unsigned char* st = stage0 + (size_t)s * L.stage_bytes;
+        const bool row_ok = t * RPS + rs < nrows;  // warp-uniform
+        const long long i = r0 + (long long)t * RPS + rs;
 
         Acc<T> ip[MCH][VEC];
 #pragma unroll
@@ -228,12 +214,28 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
 #pragma unroll
             for (int v = 0; v < VEC; ++v) ip[m][v].init();
 
-        if (ok) {
+        if (row_ok) {
+            const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
+            const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
+            const T* sS = reinterpret_cast<const T*>(slotS(st, rs) + (aS & 15));
+            const T* sX = reinterpret_cast<const T*>(slotX(st, rs) + (aX & 15));
+            T gm[MCH][VEC];
+            if (UPDATE) {
+                const uintptr_t aA = reinterpret_cast<uintptr_t>(in.psiA + i * z);
+                const T* sA = reinterpret_cast<const T*>(slotA(st, rs) + (aA & 15));
+#pragma unroll
+                for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                    for (int v = 0; v < VEC; ++v) {
+                        const long long k = (long long)(m * LPF + q) * VEC + v;
+                        gm[m][v] = (k < z) ? sAS[k] - sA[k] : T(0);
+                    }
+            }
             T sv[CPW][MCH][VEC];
             T xv[CPW];
 #pragma unroll
             for (int c = 0; c < CPW; ++c) {
-                const int jl = (warp * CPW + c) * FPW + g;
+                const int jl = (cg * CPW + c) * FPW + g;
                 const bool fv = jl < cw;
 #pragma unroll
                 for (int m = 0; m < MCH; ++m) {
@@ -250,10 +252,10 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
                 xv[c] = (UPDATE && fv) ? sX[jl] : T(0);
             }
             if (UPDATE) {
-                const T teps = T(p.eps);
+                const T teps = T(L.eps);
 #pragma unroll
                 for (int c = 0; c < CPW; ++c) {
-                    const int jl = (warp * CPW + c) * FPW + g;
+                    const int jl = (cg * CPW + c) * FPW + g;
                     const bool fv = jl < cw;
                     T sn[MCH][VEC];
                     // A fiber with X == 0 updates to zero whatever its digamma
@@ -308,10 +310,14 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
                         for (int v = 0; v < VEC; ++v) {
                             pj[c][m][v].add(sn[m][v]);
                             ip[m][v].add(sn[m][v]);
+                            if (track) {
+                                d_abs += fabs(double(sn[m][v]) - double(sv[c][m][v]));
+                                d_new += fabs(double(sn[m][v]));
+                            }
                         }
                         const long long k0 = (long long)(m * LPF + q) * VEC;
                         if (fv && k0 < z)
-                            VecIO<T, VEC>::store(p.S + ((i * p.y + c0 + jl) * z + k0), sn[m]);
+                            VecIO<T, VEC>::store(in.S + ((i * in.y + c0 + jl) * z + k0), sn[m]);
                     }
                 }
             } else {
@@ -327,7 +333,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
             }
         }
 
-        // S_ipk partial of row i over this band: fiber slots -> warp -> red[s][warp].
+        // S_ipk partial of row i over this warp's columns -> red[s][warp].
         double* redw = red + ((size_t)s * NW + warp) * z;
 #pragma unroll
         for (int m = 0; m < MCH; ++m)
@@ -339,81 +345,138 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
                 if (g == 0 && k < z) redw[k] = val;
             }
         __syncwarp();
-        // No CTA barrier per row: each warp counts itself done with stage s;
-        // the last of the NW warps (the count reaches a multiple of NW) adds the
-        // warps' partials in warp order, writes the S_ipk partial of row i and
-        // refills the stage.  Warps drift apart by up to `stages` rows.
+        // No CTA barrier per round: each warp counts itself done with stage s;
+        // the last of the NW warps (the count reaches a multiple of NW) adds, per
+        // row slot, its warps' partials in column-group order, writes the S_ipk
+        // partials of the round's rows and refills the stage.  Warps drift apart
+        // by up to `stages` rounds.
         int last = 0;
         if (lane == 0) {
             __threadfence_block();
-            last = (atomicAdd(&cnt[s], 1) == (t / p.stages + 1) * NW - 1) ? 1 : 0;
+            last = (atomicAdd(&cnt[s], 1) == (t / L.stages + 1) * NW - 1) ? 1 : 0;
         }
         last = __shfl_sync(0xffffffffu, last, 0);
         if (last) {
             __threadfence_block();
             const double* reds = red + (size_t)s * NW * z;
-            for (long long k = lane; k < z; k += 32) {
-                double sum = 0.0;
-#pragma unroll
-                for (int w = 0; w < NW; ++w) sum += reds[(size_t)w * z + k];
-                p.part_ipk[((long long)band * p.x + i) * z + k] = sum;
+            const int nr = min(RPS, nrows - t * RPS);
+            for (int r = 0; r < nr; ++r) {
+                const long long ir = r0 + (long long)t * RPS + r;
+                for (long long k = lane; k < z; k += 32) {
+                    double sum = 0.0;
+                    for (int w = 0; w < wpr; ++w) sum += reds[(size_t)(r * wpr + w) * z + k];
+                    in.part_ipk[((long long)band * in.x + ir) * z + k] = sum;
+                }
             }
             __syncwarp();
-            if (lane == 0 && t + p.stages < nrows) issue(t + p.stages);
+            if (lane == 0 && t + L.stages < nrounds) issue(t + L.stages);
         }
     }
 
-    // S_pjk partial of the band over this CTA's rows: each (j,k) has one owner.
+    // S_pjk partial of the band over this tile's rows.  With one row slot every
+    // (j,k) has a single owner lane; otherwise the row slots' partials are added
+    // in slot order through shared memory (the drained stage ring).
+    if (RPS == 1) {
 #pragma unroll
-    for (int c = 0; c < CPW; ++c) {
-        const int jl = (warp * CPW + c) * FPW + g;
+        for (int c = 0; c < CPW; ++c) {
+            const int jl = (cg * CPW + c) * FPW + g;
 #pragma unroll
-        for (int m = 0; m < MCH; ++m)
+            for (int m = 0; m < MCH; ++m)
 #pragma unroll
-            for (int v = 0; v < VEC; ++v) {
-                const long long k = (long long)(m * LPF + q) * VEC + v;
-                if (jl < cw && k < z)
-                    p.part_pjk[((long long)rr * p.y + c0 + jl) * z + k] = pj[c][m][v].value();
+                for (int v = 0; v < VEC; ++v) {
+                    const long long k = (long long)(m * LPF + q) * VEC + v;
+                    if (jl < cw && k < z)
+                        in.part_pjk[((long long)rr * in.y + c0 + jl) * z + k] = pj[c][m][v].value();
+                }
+        }
+    } else {
+        __syncthreads();  // every warp is done with the ring
+        double* pjbuf = reinterpret_cast<double*>(stage0);  // [RPS][band_w][z]
+#pragma unroll
+        for (int c = 0; c < CPW; ++c) {
+            const int jl = (cg * CPW + c) * FPW + g;
+#pragma unroll
+            for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                for (int v = 0; v < VEC; ++v) {
+                    const long long k = (long long)(m * LPF + q) * VEC + v;
+                    if (jl < in.band_w && k < z)
+                        pjbuf[((size_t)rs * in.band_w + jl) * z + k] = pj[c][m][v].value();
+                }
+        }
+        __syncthreads();
+        const long long n = (long long)cw * z;
+        for (long long e = tid; e < n; e += kSweepThreads) {
+            double sum = 0.0;
+            for (int r = 0; r < RPS; ++r) sum += pjbuf[(size_t)r * in.band_w * z + e];
+            in.part_pjk[((long long)rr * in.y + c0) * z + e] = sum;
+        }
+    }
+
+    if (track) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d_abs += __shfl_xor_sync(0xffffffffu, d_abs, o);
+            d_new += __shfl_xor_sync(0xffffffffu, d_new, o);
+        }
+        if (lane == 0) {
+            dsum[warp][0] = d_abs;
+            dsum[warp][1] = d_new;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double a = 0.0, b = 0.0;
+            for (int w = 0; w < NW; ++w) {
+                a += dsum[w][0];
+                b += dsum[w][1];
             }
+            in.delta_part[2 * tile] = a;
+            in.delta_part[2 * tile + 1] = b;
+        }
     }
 }
 
-template <typename T> struct FinParams {
-    const double* part_pjk;
-    const double* part_ipk;
-    const double* alpha;
-    const double* beta;
-    T* psiB;
-    T* psiA;
-    T* psiAS;
-    double* asum_part;
-    unsigned* counter;
-    long long x, y, z;
-    int n_rr, n_bands, nbB, n_ablk, rows_per_ablk;
-    int plus_appr, minus_appr;
-};
+template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR>
+__global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepParams<T> p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int band = blockIdx.x % p.in.n_bands;
+    const int rr = blockIdx.x / p.in.n_bands;
+    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR>(p.in, p.L, band, rr, int(blockIdx.x), smem);
+}
 
-// Blocks [0, nbB): psi(beta_eph) for every (j,k).  Blocks [nbB, nbB+n_ablk):
-// psi(alpha_eph) for a block of rows plus that block's sum of alpha_eph over
-// rows; the last block to finish sums the block sums in order and tabulates
-// psi(sum_i alpha_eph(i,k)).
+template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR>
+__global__ void __launch_bounds__(kSweepThreads, 2) sweep_batch_kernel(const BatchSweepParams<T> p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const BatchTile tl = p.tiles[blockIdx.x];
+    SweepInst<T> in = p.insts[tl.inst];
+    if (!p.track) in.delta_part = nullptr;
+    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR>(in, p.L, tl.band, tl.rr,
+                                              tl.rr * in.n_bands + tl.band, smem);
+}
+
+// Block `blk` of an instance's finalize.  Blocks [0, nbB): psi(beta_eph) for
+// every (j,k).  Blocks [nbB, nbB + n_ablk): psi(alpha_eph) for a block of rows
+// plus that block's sum of alpha_eph over rows; the last block to finish sums
+// the block sums in order, tabulates psi(sum_i alpha_eph(i,k)) and, when the
+// sweep tracked it, the relative change of S.
 template <typename T>
-__global__ void __launch_bounds__(kFinThreads) finalize_kernel(const FinParams<T> p) {
+__device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int plus_appr,
+                                               int minus_appr) {
     const long long z = p.z;
     const int tid = threadIdx.x;
-    if ((int)blockIdx.x < p.nbB) {
-        const long long idx = (long long)blockIdx.x * kFinThreads + tid;
+    if (blk < p.nbB) {
+        const long long idx = (long long)blk * kFinThreads + tid;
         if (idx < p.y * z) {
             const long long k = idx % z;
             double s = 0.0;
             for (int r = 0; r < p.n_rr; ++r) s += p.part_pjk[(long long)r * p.y * z + idx];
-            p.psiB[idx] = T(psi_mode_f64(s + p.beta[k], p.plus_appr != 0));
+            p.psiB[idx] = T(psi_mode_f64(s + p.beta[k], plus_appr != 0));
         }
         return;
     }
     __shared__ double acc[1024];
     __shared__ unsigned last;
-    const int b = (int)blockIdx.x - p.nbB;
+    const int b = blk - p.nbB;
     const long long i0 = (long long)b * p.rows_per_ablk;
     const long long i1 = min(p.x, i0 + p.rows_per_ablk);
     const int KT = (int)min(z, (long long)kFinThreads);
@@ -427,7 +490,7 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const FinParams<T
                 for (int bd = 0; bd < p.n_bands; ++bd)
                     s += p.part_ipk[((long long)bd * p.x + i) * z + k];
                 const double ae = s + p.alpha[i];
-                p.psiA[i * z + k] = T(psi_mode_f64(ae, p.minus_appr != 0));
+                p.psiA[i * z + k] = T(psi_mode_f64(ae, minus_appr != 0));
                 a += ae;
             }
             acc[sub * z + k] = a;
@@ -448,10 +511,42 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const FinParams<T
         for (long long k = tid; k < z; k += kFinThreads) {
             double a = 0.0;
             for (int bb = 0; bb < p.n_ablk; ++bb) a += __ldcg(&p.asum_part[(long long)bb * z + k]);
-            p.psiAS[k] = T(psi_mode_f64(a, p.minus_appr != 0));
+            p.psiAS[k] = T(psi_mode_f64(a, minus_appr != 0));
+        }
+        if (p.delta_part && tid == 0) {
+            double d = 0.0, n = 0.0;
+            for (int t = 0; t < p.n_tiles; ++t) {
+                d += __ldcg(&p.delta_part[2 * t]);
+                n += __ldcg(&p.delta_part[2 * t + 1]);
+            }
+            *p.rel_change = n > 0.0 ? d / n : (d > 0.0 ? 1.0 : 0.0);
         }
         if (tid == 0) *p.counter = 0u;
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kFinThreads) finalize_kernel(const FinParams<T> p) {
+    finalize_block<T>(p.f, int(blockIdx.x), p.plus_appr, p.minus_appr);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kFinThreads) finalize_batch_kernel(const BatchFinParams<T> p) {
+    // instance owning this block: last i with block_off[i] <= blockIdx.x
+    int lo = 0, hi = p.n_inst - 1;
+    const int b = int(blockIdx.x);
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.block_off[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const FinInst<T> f = p.insts[lo];
+    finalize_block<T>(f, b - p.block_off[lo], p.plus_appr, p.minus_appr);
+}
+
+void* finalize_batch_fn(int dtype) {
+    return dtype == BLDM_F64 ? reinterpret_cast<void*>(&finalize_batch_kernel<double>)
+                             : reinterpret_cast<void*>(&finalize_batch_kernel<float>);
 }
 
 // Seeded initial S: S(i,j,:) = X(i,j) * Dirichlet(1_z), the Dirichlet draw
@@ -497,41 +592,51 @@ int cuda_status(cudaError_t e) {
     } while (0)
 
 template <typename T> using SweepFn = void (*)(const SweepParams<T>);
+template <typename T> using BatchSweepFn = void (*)(const BatchSweepParams<T>);
 
 // Instantiated lane shapes: (LPF, MCH) with LPF*MCH a power of two.
-#define BLDM_SHAPE_CASES(T, VEC, UPD, APPR)                                      \
-    case 1 * 16 + 1: return &sweep_kernel<T, VEC, 1, 1, UPD, APPR>;            \
-    case 2 * 16 + 1: return &sweep_kernel<T, VEC, 2, 1, UPD, APPR>;            \
-    case 4 * 16 + 1: return &sweep_kernel<T, VEC, 4, 1, UPD, APPR>;            \
-    case 8 * 16 + 1: return &sweep_kernel<T, VEC, 8, 1, UPD, APPR>;            \
-    case 16 * 16 + 1: return &sweep_kernel<T, VEC, 16, 1, UPD, APPR>;          \
-    case 32 * 16 + 1: return &sweep_kernel<T, VEC, 32, 1, UPD, APPR>;          \
-    case 32 * 16 + 2: return &sweep_kernel<T, VEC, 32, 2, UPD, APPR>;          \
-    case 32 * 16 + 4: return &sweep_kernel<T, VEC, 32, 4, UPD, APPR>;          \
-    case 32 * 16 + 8: return &sweep_kernel<T, VEC, 32, 8, UPD, APPR>;
+#define BLDM_SHAPE_CASES(K, T, VEC, UPD, APPR)                                             \
+    case 1 * 16 + 1: return reinterpret_cast<void*>(&K<T, VEC, 1, 1, UPD, APPR>);        \
+    case 2 * 16 + 1: return reinterpret_cast<void*>(&K<T, VEC, 2, 1, UPD, APPR>);        \
+    case 4 * 16 + 1: return reinterpret_cast<void*>(&K<T, VEC, 4, 1, UPD, APPR>);        \
+    case 8 * 16 + 1: return reinterpret_cast<void*>(&K<T, VEC, 8, 1, UPD, APPR>);        \
+    case 16 * 16 + 1: return reinterpret_cast<void*>(&K<T, VEC, 16, 1, UPD, APPR>);      \
+    case 32 * 16 + 1: return reinterpret_cast<void*>(&K<T, VEC, 32, 1, UPD, APPR>);      \
+    case 32 * 16 + 2: return reinterpret_cast<void*>(&K<T, VEC, 32, 2, UPD, APPR>);      \
+    case 32 * 16 + 4: return reinterpret_cast<void*>(&K<T, VEC, 32, 4, UPD, APPR>);      \
+    case 32 * 16 + 8: return reinterpret_cast<void*>(&K<T, VEC, 32, 8, UPD, APPR>);
 
-template <typename T, int VEC, bool UPD, bool APPR> SweepFn<T> pick_shape(int lpf, int mch) {
-    switch (lpf * 16 + mch) { BLDM_SHAPE_CASES(T, VEC, UPD, APPR) default: return nullptr; }
+template <typename T, int VEC, bool UPD, bool APPR> void* pick_shape(int lpf, int mch, bool batch) {
+    if (batch) {
+        switch (lpf * 16 + mch) { BLDM_SHAPE_CASES(sweep_batch_kernel, T, VEC, UPD, APPR) default: return nullptr; }
+    }
+    switch (lpf * 16 + mch) { BLDM_SHAPE_CASES(sweep_kernel, T, VEC, UPD, APPR) default: return nullptr; }
 }
 
-template <typename T> SweepFn<T> pick_sweep(const SweepCfg& c, bool update, bool appr);
-template <> SweepFn<double> pick_sweep<double>(const SweepCfg& c, bool update, bool appr) {
-    if (c.vec == 2) {
-        if (!update) return pick_shape<double, 2, false, true>(c.lpf, c.mch);
-        return appr ? pick_shape<double, 2, true, true>(c.lpf, c.mch)
-                    : pick_shape<double, 2, true, false>(c.lpf, c.mch);
+// The sweep kernel for a lane shape: plain (one instance) or batch.  FP32 has
+// a single digamma evaluation (appr is ignored).
+void* pick_sweep_fn(int dtype, int vec, int lpf, int mch, bool update, bool appr, bool batch) {
+    if (dtype == BLDM_F64) {
+        if (vec == 2) {
+            if (!update) return pick_shape<double, 2, false, true>(lpf, mch, batch);
+            return appr ? pick_shape<double, 2, true, true>(lpf, mch, batch)
+                        : pick_shape<double, 2, true, false>(lpf, mch, batch);
+        }
+        if (!update) return pick_shape<double, 1, false, true>(lpf, mch, batch);
+        return appr ? pick_shape<double, 1, true, true>(lpf, mch, batch)
+                    : pick_shape<double, 1, true, false>(lpf, mch, batch);
     }
-    if (!update) return pick_shape<double, 1, false, true>(c.lpf, c.mch);
-    return appr ? pick_shape<double, 1, true, true>(c.lpf, c.mch)
-                : pick_shape<double, 1, true, false>(c.lpf, c.mch);
+    if (vec == 4) {
+        if (!update) return pick_shape<float, 4, false, true>(lpf, mch, batch);
+        return pick_shape<float, 4, true, true>(lpf, mch, batch);
+    }
+    if (!update) return pick_shape<float, 1, false, true>(lpf, mch, batch);
+    return pick_shape<float, 1, true, true>(lpf, mch, batch);
 }
-template <> SweepFn<float> pick_sweep<float>(const SweepCfg& c, bool update, bool) {
-    if (c.vec == 4) {
-        if (!update) return pick_shape<float, 4, false, true>(c.lpf, c.mch);
-        return pick_shape<float, 4, true, true>(c.lpf, c.mch);
-    }
-    if (!update) return pick_shape<float, 1, false, true>(c.lpf, c.mch);
-    return pick_shape<float, 1, true, true>(c.lpf, c.mch);
+
+template <typename T> SweepFn<T> pick_sweep(const SweepCfg& c, bool update, bool appr) {
+    return reinterpret_cast<SweepFn<T>>(pick_sweep_fn(sizeof(T) == 8 ? BLDM_F64 : BLDM_F32, c.vec,
+                                                      c.lpf, c.mch, update, appr, false));
 }
 
 static int pow2ceil(long v) {
@@ -548,8 +653,9 @@ static int num_sms_of(int dev) {
     return n;
 }
 
-static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int num_sms,
-                      const bldm_tuning* tune) {
+// Lane shape for depth z: VEC elements per 16-byte access when the fiber is
+// 16-byte aligned, LPF lanes per fiber, MCH chunks per lane, CPW passes.
+int lane_config(size_t z, size_t es, SweepCfg& c) {
     const bool aligned = (z * es) % 16 == 0;
     c.vec = aligned ? int(16 / es) : 1;
     const long nch = long((z + c.vec - 1) / c.vec);
@@ -562,14 +668,21 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
         if (c.mch > 8) return BLDM_ERR_UNSUPPORTED;
     }
     c.cpw = cpw_for(int(c.mch * c.vec * es));
+    return BLDM_OK;
+}
+
+static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int num_sms,
+                      const bldm_tuning* tune) {
+    if (lane_config(z, es, c) != BLDM_OK) return BLDM_ERR_UNSUPPORTED;
     c.warps = kSweepWarps;
     const int fpw = 32 / c.lpf;
-    c.band_w = c.warps * c.cpw * fpw;
+    // warps per row: as few as cover y, so that narrow rows share a stage
+    c.wpr = kSweepWarps;
+    while (c.wpr > 1 && size_t(c.wpr / 2) * c.cpw * fpw >= y) c.wpr /= 2;
+    c.band_w = c.wpr * c.cpw * fpw;
     c.n_bands = int((y + c.band_w - 1) / c.band_w);
-    c.capS = uint32_t(align_up(size_t(c.band_w) * z * es + 32, 16));
-    c.capX = uint32_t(align_up(size_t(c.band_w) * es + 32, 16));
-    c.capA = uint32_t(align_up(z * es + 32, 16));
-    c.stage_bytes = c.capS + c.capX + c.capA;
+    const SlotLayout lay(c.band_w, (long long)z, int(es));
+    c.stage_bytes = uint32_t(kSweepWarps / c.wpr) * (lay.capS + lay.capX + lay.capA);
     // each stage also owns a [warps][z] slice of S_ipk partials (FP64)
     const size_t per_stage = c.stage_bytes + size_t(kSweepWarps) * z * 8;
     const size_t fixed = 64 + z * es + 128;
@@ -593,6 +706,10 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
         if (st < 2) return BLDM_ERR_UNSUPPORTED;
     }
     c.stages = int(st);
+    // the end-of-tile S_pjk combine reuses the drained ring: [rows/stage][band_w][z]
+    if (c.wpr < kSweepWarps &&
+        size_t(kSweepWarps / c.wpr) * c.band_w * z * 8 > size_t(c.stages) * c.stage_bytes)
+        return BLDM_ERR_UNSUPPORTED;
     c.smem_update = size_t(c.stages) * per_stage + fixed;
     c.smem_sums = c.smem_update;
     c.ctas_per_sm = cps;
@@ -746,26 +863,28 @@ template <typename T>
 static SweepParams<T> sweep_params(PlanImpl* p, const void* dX, void* dS, double eps) {
     const SweepCfg& c = p->cfg;
     SweepParams<T> s;
-    s.S = static_cast<T*>(dS);
-    s.X = static_cast<const T*>(dX);
-    s.psiB = static_cast<const T*>(p->psiB);
-    s.psiA = static_cast<const T*>(p->psiA);
-    s.psiAS = static_cast<const T*>(p->psiAS);
-    s.part_pjk = p->part_pjk;
-    s.part_ipk = p->part_ipk;
-    s.err = p->err;
-    s.x = (long long)p->x;
-    s.y = (long long)p->y;
-    s.z = (long long)p->z;
-    s.n_bands = c.n_bands;
-    s.band_w = c.band_w;
-    s.rr_base = c.rr_base;
-    s.rr_extra = c.rr_extra;
-    s.stages = c.stages;
-    s.capS = c.capS;
-    s.capX = c.capX;
-    s.stage_bytes = c.stage_bytes;
-    s.eps = eps;
+    SweepInst<T>& in = s.in;
+    in.S = static_cast<T*>(dS);
+    in.X = static_cast<const T*>(dX);
+    in.psiB = static_cast<const T*>(p->psiB);
+    in.psiA = static_cast<const T*>(p->psiA);
+    in.psiAS = static_cast<const T*>(p->psiAS);
+    in.part_pjk = p->part_pjk;
+    in.part_ipk = p->part_ipk;
+    in.delta_part = nullptr;
+    in.x = (long long)p->x;
+    in.y = (long long)p->y;
+    in.z = (long long)p->z;
+    in.n_bands = c.n_bands;
+    in.band_w = c.band_w;
+    in.wpr = c.wpr;
+    in.n_rr = c.n_rr;
+    in.rr_base = c.rr_base;
+    in.rr_extra = c.rr_extra;
+    s.L.stages = c.stages;
+    s.L.stage_bytes = c.stage_bytes;
+    s.L.eps = eps;
+    s.L.err = p->err;
     return s;
 }
 
@@ -773,7 +892,8 @@ template <typename T>
 static FinParams<T> fin_params(PlanImpl* p, const double* dalpha, const double* dbeta,
                                int plus_appr, int minus_appr) {
     const SweepCfg& c = p->cfg;
-    FinParams<T> f;
+    FinParams<T> fp;
+    FinInst<T>& f = fp.f;
     f.part_pjk = p->part_pjk;
     f.part_ipk = p->part_ipk;
     f.alpha = dalpha;
@@ -783,6 +903,8 @@ static FinParams<T> fin_params(PlanImpl* p, const double* dalpha, const double* 
     f.psiAS = static_cast<T*>(p->psiAS);
     f.asum_part = p->asum_part;
     f.counter = p->counter;
+    f.delta_part = nullptr;
+    f.rel_change = nullptr;
     f.x = (long long)p->x;
     f.y = (long long)p->y;
     f.z = (long long)p->z;
@@ -791,9 +913,10 @@ static FinParams<T> fin_params(PlanImpl* p, const double* dalpha, const double* 
     f.nbB = int((p->y * p->z + kFinThreads - 1) / kFinThreads);
     f.n_ablk = c.n_ablk;
     f.rows_per_ablk = c.rows_per_ablk;
-    f.plus_appr = plus_appr;
-    f.minus_appr = minus_appr;
-    return f;
+    f.n_tiles = c.n_rr * c.n_bands;
+    fp.plus_appr = plus_appr;
+    fp.minus_appr = minus_appr;
+    return fp;
 }
 
 template <typename T>
@@ -809,7 +932,7 @@ static int run_typed(PlanImpl* p, const void* dX, const double* dalpha, const do
     const SweepParams<T> sp = sweep_params<T>(p, dX, dS, eps);
     const FinParams<T> fp = fin_params<T>(p, dalpha, dbeta, plus_appr, minus_appr);
     const dim3 grid_s(unsigned(c.n_bands) * unsigned(c.n_rr));
-    const dim3 grid_f(unsigned(fp.nbB + fp.n_ablk));
+    const dim3 grid_f(unsigned(fp.f.nbB + fp.f.n_ablk));
     fsum<<<grid_s, kSweepThreads, c.smem_sums, st>>>(sp);
     finalize_kernel<T><<<grid_f, kFinThreads, 0, st>>>(fp);
     p->launches += 2;
@@ -851,6 +974,18 @@ int plan_init_S(PlanImpl* p, const void* dX, void* dS, uint64_t seed, cudaStream
                                                      static_cast<float*>(dS), nf,
                                                      (long long)p->z, seed);
     p->launches += 1;
+    return cuda_status(cudaGetLastError());
+}
+
+int launch_init_S(int dtype, const void* dX, void* dS, long long nf, long long z, uint64_t seed,
+                  cudaStream_t st) {
+    const unsigned blocks = unsigned((nf + 255) / 256);
+    if (dtype == BLDM_F64)
+        init_S_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(dX),
+                                                      static_cast<double*>(dS), nf, z, seed);
+    else
+        init_S_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const float*>(dX),
+                                                     static_cast<float*>(dS), nf, z, seed);
     return cuda_status(cudaGetLastError());
 }
 

@@ -238,6 +238,38 @@ int bldm_log_marginal_S(const void* d_S, int dtype, size_t x, size_t y, size_t z
                         const double* alpha, const double* beta, double a,
                         double b, double* result, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched solver: many independent instances of different shapes (x, y, z
+ * each) solved together.  No counterpart in the reference, which solves one
+ * instance per call; each instance's result is the one bldm_plan_run gives
+ * for it alone (same tiling, same reduction order).  One iteration of every
+ * instance is one fused-sweep launch per lane-shape class (instances whose z
+ * maps to the same kernel), the classes concurrent on forked streams, and one
+ * finalize launch for all instances; with use_graph the whole run is captured
+ * once per (iters, psi_mode, eps) into a CUDA graph and replayed.
+ * rows_per_tile (0 = 64) sets the rows of one CTA tile (the autotuner's knob).
+ * X, S0 and S_out are host FP64 arrays (converted for BLDM_F32 storage).
+ * ---------------------------------------------------------------------- */
+typedef struct bldm_batch bldm_batch;
+int bldm_batch_create(bldm_batch** batch, int dtype, size_t n, const size_t* xs,
+                      const size_t* ys, const size_t* zs, int rows_per_tile);
+int bldm_batch_destroy(bldm_batch* batch);
+/* Instance idx's data; S0 NULL draws the seeded initial S on the device. */
+int bldm_batch_set(bldm_batch* batch, size_t idx, const double* X, const double* alpha,
+                   const double* beta, const double* S0, uint64_t seed);
+/* Runs `iters` iterations of every instance from its current S (asynchronous
+ * on `stream`; use_graph needs a non-NULL stream). */
+int bldm_batch_run(bldm_batch* batch, size_t iters, int psi_mode, double eps,
+                   int use_graph, void* stream);
+int bldm_batch_check(bldm_batch* batch, void* stream);
+/* Instance idx's S (x*y*z) and the relative change sum|S_n - S_{n-1}| /
+ * sum|S_n| of the run's last iteration; either output may be NULL. */
+int bldm_batch_get(bldm_batch* batch, size_t idx, double* S_out, double* rel_change);
+/* Device buffers of instance idx (storage dtype), for device-resident callers. */
+int bldm_batch_device_ptrs(bldm_batch* batch, size_t idx, void** d_X, void** d_S);
+int bldm_batch_info(const bldm_batch* batch, size_t* n_classes, size_t* device_bytes,
+                    uint64_t* launches);
+
 /* Library version string. */
 const char* bldm_version(void);
 

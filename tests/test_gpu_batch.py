@@ -1,0 +1,146 @@
+"""GPU tests of the batched solver (bldm_batch_*): many instances of different
+shapes in shared launches.  Tolerances as in test_gpu_parity: FP64 within 1e-9
+(max-norm relative) of the oracle; FP32 storage within 1e-5, or 10x the FP32
+restatement's own error where that is larger.  An instance's result must not
+depend on the batch it is solved in (bitwise)."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(64, 48, 8), (33, 65, 3), (96, 80, 16), (130, 70, 8), (40, 41, 64), (7, 300, 5),
+          (32, 32, 4), (200, 150, 32), (5, 7, 17), (70, 33, 4), (128, 256, 16), (48, 64, 64)]
+
+
+def rel_err(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _problems(workloads, oracle, shapes, seed0=0):
+    out = []
+    for k, (x, y, z) in enumerate(shapes):
+        rng = np.random.default_rng(seed0 + k)
+        X = workloads.allocation_model_X(x, y, z, 5.0, 0.05, rng) + rng.poisson(1.0, (x, y))
+        alpha = rng.uniform(1.0, 2.0, x)
+        beta = rng.uniform(1.0, 2.0, z)
+        out.append((X, alpha, beta, oracle.init_S(X, z, seed0 + k)))
+    return out
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_fp64_matches_oracle(bldm, oracle, workloads, use_graph):
+    probs = _problems(workloads, oracle, SHAPES)
+    b = bldm.Batch(SHAPES, dtype=bldm.F64)
+    for k, (X, a, be, S0) in enumerate(probs):
+        b.set(k, X, a, be, S0)
+    import torch
+    stream = torch.cuda.Stream()
+    b.run(15, bldm.PSI_APPR, use_graph=use_graph, stream=stream)
+    b.check(stream)
+    for k, (X, a, be, S0) in enumerate(probs):
+        ref = oracle.bld_mult(X, SHAPES[k][2], a, be, 15, oracle.PSI_APPR, 1e-50, S0=S0)
+        S, _ = b.get(k)
+        assert rel_err(S, ref) <= 1e-9, (SHAPES[k], rel_err(S, ref))
+    info = b.info()
+    assert info["classes"] >= 5
+    b.close()
+
+
+def test_batch_modes_exact_and_legacy(bldm, oracle, workloads):
+    shapes = SHAPES[:4]
+    probs = _problems(workloads, oracle, shapes, 100)
+    for mode in (bldm.PSI_EXACT, bldm.PSI_LEGACY_CUDA):
+        b = bldm.Batch(shapes, dtype=bldm.F64)
+        for k, (X, a, be, S0) in enumerate(probs):
+            b.set(k, X, a, be, S0)
+        b.run(10, mode, use_graph=False)
+        b.check()
+        for k, (X, a, be, S0) in enumerate(probs):
+            ref = oracle.bld_mult(X, shapes[k][2], a, be, 10, mode, 1e-50, S0=S0)
+            assert rel_err(b.get(k)[0], ref) <= 1e-9
+        b.close()
+
+
+def test_instance_alone_equals_instance_in_mix(bldm, oracle, workloads):
+    probs = _problems(workloads, oracle, SHAPES, 7)
+    mix = bldm.Batch(SHAPES, dtype=bldm.F32)
+    for k, (X, a, be, S0) in enumerate(probs):
+        mix.set(k, X, a, be, S0)
+    mix.run(20, use_graph=True, stream=None)
+    mix.check()
+    for k in (0, 4, 7, 11):
+        alone = bldm.Batch([SHAPES[k]], dtype=bldm.F32)
+        X, a, be, S0 = probs[k]
+        alone.set(0, X, a, be, S0)
+        alone.run(20, use_graph=False)
+        alone.check()
+        Sa, ra = alone.get(0)
+        Sm, rm = mix.get(k)
+        np.testing.assert_array_equal(Sa, Sm)
+        assert ra == rm
+        alone.close()
+    mix.close()
+
+
+def test_batch_fp32_vs_fp64(bldm, oracle, workloads):
+    probs = _problems(workloads, oracle, SHAPES, 20)
+    b = bldm.Batch(SHAPES, dtype=bldm.F32)
+    for k, (X, a, be, S0) in enumerate(probs):
+        b.set(k, X, a, be, S0)
+    b.run(12, use_graph=False)
+    b.check()
+    for k, (X, a, be, S0) in enumerate(probs):
+        z = SHAPES[k][2]
+        ref = oracle.bld_mult(X, z, a, be, 12, oracle.PSI_APPR, 1e-50, S0=S0)
+        ref32 = oracle.bld_mult(X, z, a, be, 12, oracle.PSI_APPR, 1e-50, S0=S0, dtype=np.float32)
+        S, _ = b.get(k)
+        assert np.all(np.isfinite(S))
+        assert rel_err(S, ref) <= max(1e-5, 10 * rel_err(ref32, ref)), SHAPES[k]
+    b.close()
+
+
+def test_batch_relative_change(bldm, oracle, workloads):
+    shapes = [(60, 50, 8), (30, 90, 16)]
+    probs = _problems(workloads, oracle, shapes, 40)
+    b = bldm.Batch(shapes, dtype=bldm.F64)
+    for k, (X, a, be, S0) in enumerate(probs):
+        b.set(k, X, a, be, S0)
+    b.run(6, use_graph=False)
+    b.check()
+    for k, (X, a, be, S0) in enumerate(probs):
+        s5 = oracle.bld_mult(X, shapes[k][2], a, be, 5, oracle.PSI_APPR, 1e-50, S0=S0)
+        s6 = oracle.bld_mult(X, shapes[k][2], a, be, 6, oracle.PSI_APPR, 1e-50, S0=S0)
+        ref = np.abs(s6 - s5).sum() / np.abs(s6).sum()
+        S, rel = b.get(k)
+        assert abs(rel - ref) <= 1e-9 * ref + 1e-15
+    # a second run continues from the current S
+    b.run(2, use_graph=False)
+    b.check()
+    s8 = oracle.bld_mult(probs[0][0], 8, probs[0][1], probs[0][2], 8, oracle.PSI_APPR, 1e-50,
+                         S0=probs[0][3])
+    assert rel_err(b.get(0)[0], s8) <= 1e-9
+    b.close()
+
+
+def test_batch_seeded_init_matches_oracle(bldm, oracle):
+    rng = np.random.default_rng(3)
+    X = rng.poisson(3.0, (20, 30)).astype(float)
+    b = bldm.Batch([(20, 30, 6)], dtype=bldm.F64)
+    b.set(0, X, np.ones(20), np.ones(6), None, seed=99)
+    b.run(3, use_graph=False)
+    ref = oracle.bld_mult(X, 6, np.ones(20), np.ones(6), 3, oracle.PSI_APPR, 1e-50,
+                          S0=oracle.init_S(X, 6, 99))
+    assert rel_err(b.get(0)[0], ref) <= 1e-9
+    b.close()
+
+
+def test_batch_rejects_bad_input(bldm):
+    b = bldm.Batch([(4, 5, 3)], dtype=bldm.F64)
+    X = np.ones((4, 5))
+    X[0, 0] = -1
+    with pytest.raises(ValueError):
+        b.set(0, X, np.ones(4), np.ones(3))
+    with pytest.raises(ValueError):
+        b.set(3, np.ones((4, 5)), np.ones(4), np.ones(3))
+    b.close()
