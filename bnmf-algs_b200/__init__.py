@@ -72,6 +72,26 @@ class bldm_stats(ctypes.Structure):
                 ("rel_change", ctypes.c_double)]
 
 
+class bldm_server_config(ctypes.Structure):
+    _fields_ = [("dtype", ctypes.c_int), ("psi_mode", ctypes.c_int), ("eps", ctypes.c_double),
+                ("tol", ctypes.c_double), ("max_iter", ctypes.c_size_t),
+                ("iters_per_round", ctypes.c_size_t), ("max_active", ctypes.c_size_t),
+                ("memory_budget", ctypes.c_size_t), ("rows_per_tile", ctypes.c_int)]
+
+
+class bldm_request_stats(ctypes.Structure):
+    _fields_ = [("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("iterations", ctypes.c_uint64), ("rel_change", ctypes.c_double),
+                ("log_marginal", ctypes.c_double), ("status", ctypes.c_int)]
+
+
+class bldm_server_stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("submitted", "completed", "failed", "rounds",
+                                              "iterations")] + \
+               [(n, ctypes.c_size_t) for n in ("active", "queued", "bytes_in_use", "bytes_peak",
+                                              "budget")]
+
+
 _lib = None
 _vp = ctypes.c_void_p
 _sz = ctypes.c_size_t
@@ -148,6 +168,16 @@ SIGNATURES = {
                                               ctypes.POINTER(_vp)]),
     "bldm_batch_info": (ctypes.c_int, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz),
                                        ctypes.POINTER(ctypes.c_uint64)]),
+    "bldm_server_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.POINTER(bldm_server_config)]),
+    "bldm_server_destroy": (ctypes.c_int, [_vp]),
+    "bldm_server_submit": (ctypes.c_int, [_vp, _dp, _sz, _sz, _sz, ctypes.POINTER(bldm_params),
+                                          ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    "bldm_server_poll": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]),
+    "bldm_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_double]),
+    "bldm_server_fetch": (ctypes.c_int, [_vp, ctypes.c_uint64, _dp,
+                                         ctypes.POINTER(bldm_request_stats)]),
+    "bldm_server_cancel": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "bldm_server_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(bldm_server_stats)]),
     "bldm_version": (ctypes.c_char_p, []),
 }
 
@@ -450,3 +480,68 @@ class Batch:
         _check(lib().bldm_batch_info(self._h, ctypes.byref(nc), ctypes.byref(nb),
                                      ctypes.byref(nl)))
         return {"classes": nc.value, "device_bytes": nb.value, "launches": nl.value}
+
+
+class Server:
+    """bldm_server: continuous batching of solves; S stays on the device between rounds."""
+
+    QUEUED, ACTIVE, DONE, FAILED = 0, 1, 2, 3
+
+    def __init__(self, dtype=F32, psi_mode=PSI_APPR, eps=1e-50, tol=1e-6, max_iter=500,
+                 iters_per_round=10, max_active=256, memory_budget=0, rows_per_tile=0):
+        cfg = bldm_server_config(dtype, psi_mode, eps, tol, max_iter, iters_per_round, max_active,
+                                 memory_budget, rows_per_tile)
+        self.dtype = dtype
+        self._h = ctypes.c_void_p()
+        self._shapes = {}
+        _check(lib().bldm_server_create(ctypes.byref(self._h), ctypes.byref(cfg)),
+               "server_create")
+
+    def close(self):
+        if self._h:
+            lib().bldm_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, X, z, params, seed=0):
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        x, y = X.shape
+        cp = params.c_struct()
+        rid = ctypes.c_uint64()
+        _check(lib().bldm_server_submit(self._h, X.ctypes.data_as(_dp), x, y, int(z),
+                                        ctypes.byref(cp), int(seed), ctypes.byref(rid)),
+               "server_submit")
+        self._shapes[rid.value] = (x, y, int(z))
+        return rid.value
+
+    def poll(self, rid):
+        st = ctypes.c_int()
+        _check(lib().bldm_server_poll(self._h, rid, ctypes.byref(st)))
+        return st.value
+
+    def wait(self, rid, timeout=120.0):
+        return lib().bldm_server_wait(self._h, rid, float(timeout)) == OK
+
+    def fetch(self, rid):
+        """(S or None, stats dict); S is None when the request failed."""
+        x, y, z = self._shapes.pop(rid)
+        S = np.empty((x, y, z))
+        rs = bldm_request_stats()
+        rc = lib().bldm_server_fetch(self._h, rid, S.ctypes.data_as(_dp), ctypes.byref(rs))
+        stats = {"queue_ms": rs.queue_ms, "latency_ms": rs.latency_ms,
+                 "iterations": rs.iterations, "rel_change": rs.rel_change,
+                 "log_marginal": rs.log_marginal, "status": rs.status}
+        return (S if rc == OK else None), stats
+
+    def cancel(self, rid):
+        _check(lib().bldm_server_cancel(self._h, rid))
+
+    def stats(self):
+        st = bldm_server_stats()
+        _check(lib().bldm_server_get_stats(self._h, ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in bldm_server_stats._fields_}

@@ -238,8 +238,8 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
             for (int ap = 0; ap < 2; ++ap) {
                 void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, upd != 0, ap != 0, true);
                 if (!fn) return BLDM_ERR_UNSUPPORTED;
-                ENG_CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(k.smem)));
+                const int rc_attr = ensure_smem_attr(fn, k.smem);
+                if (rc_attr) return rc_attr;
             }
     }
     // Tiles of every instance, per class.

@@ -67,5 +67,6 @@ int plan_check(PlanImpl* p, cudaStream_t st);
 
 int cuda_status(cudaError_t e);
 int lane_config(size_t z, size_t es, SweepCfg& c);
+int ensure_smem_attr(void* fn, size_t bytes);
 
 }  // namespace bldm

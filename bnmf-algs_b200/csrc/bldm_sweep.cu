@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 #include "bldm_device.cuh"
@@ -71,7 +72,7 @@ __device__ __forceinline__ uintptr_t align_up16(uintptr_t a) {
 // lane = g*LPF + q handles fiber slot g of its warp and elements
 // k = (m*LPF + q)*VEC + v; warp w works on row slot w / wpr and column group
 // w % wpr of the band.
-template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR>
+template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool BATCH>
 __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLaunch& L, int band,
                                            int rr, int tile, unsigned char* smem) {
     constexpr int NW = kSweepWarps;
@@ -185,7 +186,8 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             }
         }
     }
-    const bool track = UPDATE && in.delta_part != nullptr;
+    // only multi-instance sweeps track the relative change
+    const bool track = BATCH && UPDATE && in.delta_part != nullptr;
     double d_abs = 0.0, d_new = 0.0;
 
     for (int t = 0; t < nrounds; ++t) {
@@ -362,9 +364,15 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             const int nr = min(RPS, nrows - t * RPS);
             for (int r = 0; r < nr; ++r) {
                 const long long ir = r0 + (long long)t * RPS + r;
+                const double* redr = reds + (size_t)r * wpr * z;
                 for (long long k = lane; k < z; k += 32) {
+                    // all loads issued together; warps beyond wpr add nothing
+                    double part[NW];
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) part[w] = w < wpr ? redr[(size_t)w * z + k] : 0.0;
                     double sum = 0.0;
-                    for (int w = 0; w < wpr; ++w) sum += reds[(size_t)(r * wpr + w) * z + k];
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) sum += part[w];
                     in.part_ipk[((long long)band * in.x + ir) * z + k] = sum;
                 }
             }
@@ -441,7 +449,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepPara
     extern __shared__ __align__(128) unsigned char smem[];
     const int band = blockIdx.x % p.in.n_bands;
     const int rr = blockIdx.x / p.in.n_bands;
-    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR>(p.in, p.L, band, rr, int(blockIdx.x), smem);
+    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR, false>(p.in, p.L, band, rr, int(blockIdx.x), smem);
 }
 
 template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR>
@@ -450,8 +458,8 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_batch_kernel(const Bat
     const BatchTile tl = p.tiles[blockIdx.x];
     SweepInst<T> in = p.insts[tl.inst];
     if (!p.track) in.delta_part = nullptr;
-    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR>(in, p.L, tl.band, tl.rr,
-                                              tl.rr * in.n_bands + tl.band, smem);
+    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR, true>(in, p.L, tl.band, tl.rr,
+                                                    tl.rr * in.n_bands + tl.band, smem);
 }
 
 // Block `blk` of an instance's finalize.  Blocks [0, nbB): psi(beta_eph) for
@@ -583,6 +591,24 @@ int cuda_status(cudaError_t e) {
     if (e == cudaErrorMemoryAllocation) return BLDM_ERR_OOM;
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return BLDM_ERR_NO_DEVICE;
     return BLDM_ERR_CUDA;
+}
+
+// The max-dynamic-shared-memory attribute belongs to the kernel function, not
+// to a launch: plans and batches of different shapes share kernels, so the
+// attribute only ever grows (a smaller value would break an earlier plan).
+int ensure_smem_attr(void* fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, void*>, size_t> set;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = set[std::make_pair(dev, fn)];
+    if (bytes <= cur) return BLDM_OK;
+    const cudaError_t e =
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (e != cudaSuccess) return cuda_status(e);
+    cur = bytes;
+    return BLDM_OK;
 }
 
 #define BLDM_CU(call)                                   \
@@ -786,8 +812,8 @@ int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_
             else
                 fn = reinterpret_cast<void*>(pick_sweep<float>(c, upd != 0, ap != 0));
             if (!fn) return BLDM_ERR_UNSUPPORTED;
-            BLDM_CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(c.smem_update)));
+            const int rc_attr = ensure_smem_attr(fn, c.smem_update);
+            if (rc_attr) return rc_attr;
         }
     return BLDM_OK;
 }
@@ -848,8 +874,8 @@ int plan_setup_in(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, void* ws
             else
                 fn = reinterpret_cast<void*>(pick_sweep<float>(c, upd != 0, ap != 0));
             if (!fn) return BLDM_ERR_UNSUPPORTED;
-            BLDM_CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(c.smem_update)));
+            const int rc_attr = ensure_smem_attr(fn, c.smem_update);
+            if (rc_attr) return rc_attr;
         }
     return BLDM_OK;
 }

@@ -270,6 +270,61 @@ int bldm_batch_device_ptrs(bldm_batch* batch, size_t idx, void** d_X, void** d_S
 int bldm_batch_info(const bldm_batch* batch, size_t* n_classes, size_t* device_bytes,
                     uint64_t* launches);
 
+/* ------------------------------------------------------------------------
+ * Serving loop with continuous batching.  No counterpart in the reference.
+ * A worker thread admits submitted requests while a slot (max_active) and
+ * device memory (memory_budget bytes, 0 = 80% of the free memory at create,
+ * and the device's current free memory) allow, keeps each request's X, S and
+ * tables on the device, runs iters_per_round iterations of all active
+ * requests per round in shared launches, and retires a request when the
+ * relative change of S (sum|S_n - S_{n-1}| / sum|S_n| over its last
+ * iteration) falls below tol or it has run max_iter iterations (rounded up to
+ * a whole round).  Retirement copies S to the host and computes
+ * log_marginal_S on the device (FP64).  A request's result does not depend
+ * on the other requests being served.
+ * ---------------------------------------------------------------------- */
+typedef struct bldm_server bldm_server;
+typedef struct bldm_server_config {
+    int dtype;               /* BLDM_F64 or BLDM_F32 storage */
+    int psi_mode;            /* bldm_psi_mode */
+    double eps;              /* the reference's eps (1e-50) */
+    double tol;              /* retire when the relative change of S < tol */
+    size_t max_iter;         /* iteration cap per request */
+    size_t iters_per_round;  /* iterations between admission/retirement points */
+    size_t max_active;       /* concurrent requests on the device */
+    size_t memory_budget;    /* device bytes for requests; 0 = 80% of free */
+    int rows_per_tile;       /* 0 = 64 */
+} bldm_server_config;
+typedef struct bldm_request_stats {
+    double queue_ms;         /* submit -> admission */
+    double latency_ms;       /* submit -> result ready */
+    uint64_t iterations;
+    double rel_change;       /* relative change of S at retirement */
+    double log_marginal;     /* log_marginal_S of the result (FP64) */
+    int status;              /* bldm_status of the request */
+} bldm_request_stats;
+typedef struct bldm_server_stats {
+    uint64_t submitted, completed, failed, rounds, iterations;
+    size_t active, queued, bytes_in_use, bytes_peak, budget;
+} bldm_server_stats;
+int bldm_server_create(bldm_server** server, const bldm_server_config* config);
+/* Stops the worker; requests still active or queued are dropped. */
+int bldm_server_destroy(bldm_server* server);
+/* Queues a request (X host x*y, copied); BLDM_ERR_TOO_LARGE if it can never
+ * fit the memory budget. */
+int bldm_server_submit(bldm_server* server, const double* X, size_t x, size_t y, size_t z,
+                       const bldm_params* params, uint64_t seed, uint64_t* request_id);
+/* state: 0 queued, 1 active, 2 done, 3 failed. */
+int bldm_server_poll(bldm_server* server, uint64_t request_id, int* state);
+/* Blocks until the request is done or failed (BLDM_ERR_BUSY on timeout). */
+int bldm_server_wait(bldm_server* server, uint64_t request_id, double timeout_s);
+/* Copies the result (x*y*z FP64 host; may be NULL) and stats, then forgets
+ * the request; returns the request's status. */
+int bldm_server_fetch(bldm_server* server, uint64_t request_id, double* S_out,
+                      bldm_request_stats* stats);
+int bldm_server_cancel(bldm_server* server, uint64_t request_id);
+int bldm_server_get_stats(bldm_server* server, bldm_server_stats* stats);
+
 /* Library version string. */
 const char* bldm_version(void);
 
