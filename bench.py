@@ -422,6 +422,85 @@ def run_batch(args):
     return 0
 
 
+def run_serve(args):
+    """Continuous-batching server under Poisson arrivals."""
+    import threading
+    import torch
+    pkg = load_package()
+    import bnmf_algs_b200.workloads as W
+    rng = np.random.default_rng(11)
+    # request templates: the batch size distribution plus the 4096x4096x32 tail
+    reg = [W.batch_instance(s, 5000 + k) for k, s in enumerate(W.batch_shapes(96, 21))]
+    tail = [W.batch_instance((4096, 4096, 32), 9000 + k) for k in range(2)]
+    n_max = int(args.rate * args.duration * 1.5) + 16
+    times, _ = W.serving_requests(n_max, args.rate, seed=4)
+    times = times[times < args.duration]
+    picks = []
+    for _ in range(len(times)):
+        picks.append(tail[rng.integers(len(tail))] if rng.random() < 0.02
+                     else reg[rng.integers(len(reg))])
+    dtype = pkg.F64 if args.dtype == "f64" else pkg.F32
+    srv = pkg.Server(dtype=dtype, tol=1e-6, max_iter=500, iters_per_round=10, max_active=256)
+    ids = []
+    t0 = time.perf_counter()
+    with ClockSampler(0) as clk:
+        for k, (t, pr) in enumerate(zip(times, picks)):
+            now = time.perf_counter() - t0
+            if t > now:
+                time.sleep(t - now)
+            rid = srv.submit(pr["X"], pr["z"], pkg.Params(pr["a"], pr["b"], pr["alpha"],
+                                                          pr["beta"]), seed=k)
+            ids.append((rid, k, pr))
+        results = []
+        for rid, k, pr in ids:
+            srv.wait(rid, 600.0)
+            S, st = srv.fetch(rid)
+            results.append((k, pr, S, st))
+    wall = time.perf_counter() - t0
+    sstats = srv.stats()
+    srv.close()
+    ok = [r for r in results if r[3]["status"] == 0]
+    lat = np.array([r[3]["latency_ms"] for r in ok])
+    tail_lat = np.array([r[3]["latency_ms"] for r in ok if r[1]["X"].shape == (4096, 4096)])
+    reg_lat = np.array([r[3]["latency_ms"] for r in ok if r[1]["X"].shape != (4096, 4096)])
+    iters = np.array([r[3]["iterations"] for r in ok])
+    upd = sum(r[1]["X"].size * r[1]["z"] * r[3]["iterations"] for r in ok)
+    # per-request log-marginal error vs an FP64 solve of the same request
+    errs = []
+    sample = [r for r in ok if r[1]["X"].shape != (4096, 4096)][: args.fp64_sample]
+    for k, pr, S, st in sample:
+        x, y = pr["X"].shape
+        z = pr["z"]
+        plan = pkg.Plan(x, y, z, pkg.F64)
+        dX = torch.as_tensor(pr["X"]).cuda()
+        dS = torch.empty((x, y, z), dtype=torch.float64, device="cuda")
+        plan.init_S(dX, dS, seed=k)
+        plan.run(dX, torch.as_tensor(pr["alpha"]).cuda(), torch.as_tensor(pr["beta"]).cuda(),
+                 dS, int(st["iterations"]), pkg.PSI_APPR)
+        plan.check()
+        lm64 = pkg.log_marginal_S(dS, pkg.Params(pr["a"], pr["b"], pr["alpha"], pr["beta"]))
+        errs.append(abs(st["log_marginal"] - lm64) / abs(lm64))
+        plan.close()
+    pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None
+    line = {"metric": "serving_latency_p50_p99", "value": pct(lat, 50), "unit": "ms (p50)",
+            "p99_ms": pct(lat, 99), "n_gpus": 1, "higher_is_better": False,
+            "dtype": args.dtype, "data": "synthetic",
+            "config": {"workload": "serving_poisson", "offered_rate_per_s": args.rate,
+                       "duration_s": args.duration, "tol": 1e-6, "max_iter": 500,
+                       "iters_per_round": 10, "sizes": "batch distribution + 2% 4096x4096x32"},
+            "requests": len(results), "completed": len(ok), "solves_per_s": len(ok) / wall,
+            "S_updates_per_s": upd / wall, "wall_s": wall,
+            "regular_p50_ms": pct(reg_lat, 50), "regular_p99_ms": pct(reg_lat, 99),
+            "tail_requests": int(len(tail_lat)), "tail_p50_ms": pct(tail_lat, 50),
+            "iterations_p50": pct(iters, 50), "iterations_max": int(iters.max()) if len(iters) else 0,
+            "log_marginal_rel_err_vs_fp64": {"max": max(errs) if errs else None,
+                                             "median": float(np.median(errs)) if errs else None,
+                                             "n": len(errs)},
+            "server": sstats, "clocks": clk.summary()}
+    print(json.dumps(line))
+    return 0
+
+
 def make_X(kind, x, y, z, rng):
     """X kinds: 'model' (the plain workload's allocation-model draw), 'dense'
     (1 + Poisson(10), no zeros), 'zeros' (all zero)."""
@@ -476,7 +555,9 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--dtype", choices=["f64", "f32"], default="f64")
+    ap.add_argument("--dtype", choices=["f64", "f32"], default=None,
+                    help="storage precision (default f64 for the plain solve, f32 for --batch "
+                         "and --serve)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
@@ -490,6 +571,12 @@ def main():
                          "z in {4..64}, FP32, 150 iterations; vs a loop of the plain solver")
     ap.add_argument("--batch-n", type=int, default=512)
     ap.add_argument("--rows-per-tile", type=int, default=0)
+    ap.add_argument("--serve", action="store_true",
+                    help="serving loop: Poisson arrivals at --rate req/s for --duration s; "
+                         "p50/p99 latency, solves/s, log-marginal error vs FP64")
+    ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--duration", type=float, default=20.0)
+    ap.add_argument("--fp64-sample", type=int, default=16)
     ap.add_argument("--kernel-matrix", action="store_true",
                     help="time the update sweep (CUDA events) over X kinds, dtypes and launch "
                          "knobs; one JSON line each")
@@ -500,8 +587,12 @@ def main():
         return run_kernel_matrix(args)
     if args.batch:
         return run_batch(args)
+    if args.serve:
+        return run_serve(args)
     if args.warmup < 3:
         args.warmup = 3
+    if args.dtype is None:
+        args.dtype = "f32" if (args.batch or args.serve) else "f64"
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

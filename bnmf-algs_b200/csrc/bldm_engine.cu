@@ -197,11 +197,14 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
     old.swap(classes_);
     auto class_of = [&](const SweepCfg& c) -> ShapeClass& {
         for (auto& k : classes_)
-            if (k.vec == c.vec && k.lpf == c.lpf && k.mch == c.mch) return k;
+            if (k.vec == c.vec && k.lpf == c.lpf && k.mch == c.mch &&
+                k.multirow == (c.wpr < kSweepWarps))
+                return k;
         ShapeClass k;
         k.vec = c.vec;
         k.lpf = c.lpf;
         k.mch = c.mch;
+        k.multirow = c.wpr < kSweepWarps;
         classes_.push_back(k);
         return classes_.back();
     };
@@ -236,7 +239,8 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
         k.smem = size_t(k.stages) * per_stage + fixed;
         for (int upd = 0; upd < 2; ++upd)
             for (int ap = 0; ap < 2; ++ap) {
-                void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, upd != 0, ap != 0, true);
+                void* fn =
+                    pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, upd != 0, ap != 0, true, k.multirow);
                 if (!fn) return BLDM_ERR_UNSUPPORTED;
                 const int rc_attr = ensure_smem_attr(fn, k.smem);
                 if (rc_attr) return rc_attr;
@@ -314,7 +318,7 @@ int Engine::launch_sweeps(bool update, bool appr, bool track, double eps, cudaSt
         if (k.tiles.empty()) continue;
         cudaStream_t s = fork ? k.stream : st;
         if (fork) ENG_CU(cudaStreamWaitEvent(s, fork_, 0));
-        void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, update, appr, true);
+        void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, update, appr, true, k.multirow);
         if (dtype_ == BLDM_F64)
             launch_class_kernel<double>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_,
                                         k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track);

@@ -79,6 +79,7 @@ class Engine {
   private:
     struct ShapeClass {
         int vec, lpf, mch;
+        bool multirow;  // instances with fewer than 8 warps per row
         size_t max_z = 0;
         uint32_t stage_bytes = 0;
         int stages = 0;

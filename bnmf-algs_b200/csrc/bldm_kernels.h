@@ -101,8 +101,13 @@ template <typename T> struct BatchFinParams {
 };
 
 // Kernel entry points by lane shape (defined in bldm_sweep.cu).
-void* pick_sweep_fn(int dtype, int vec, int lpf, int mch, bool update, bool appr, bool batch);
+void* pick_sweep_fn(int dtype, int vec, int lpf, int mch, bool update, bool appr, bool batch,
+                    bool multirow);
 void* finalize_batch_fn(int dtype);
+void* pick_sweep_f64_plain(int vec, int lpf, int mch, bool update, bool appr, bool mr);
+void* pick_sweep_f64_batch(int vec, int lpf, int mch, bool update, bool appr, bool mr);
+void* pick_sweep_f32_plain(int vec, int lpf, int mch, bool update, bool mr);
+void* pick_sweep_f32_batch(int vec, int lpf, int mch, bool update, bool mr);
 int launch_init_S(int dtype, const void* dX, void* dS, long long nf, long long z, uint64_t seed,
                   cudaStream_t st);
 

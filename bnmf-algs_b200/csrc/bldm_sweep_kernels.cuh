@@ -1,0 +1,446 @@
+// The fused sweep kernels (templates).  Instantiated by lane shape in
+// bldm_pick_{f64,f32}_{plain,batch}.cu so that they compile in parallel.
+#pragma once
+
+#include "bldm_device.cuh"
+#include "bldm_kernels.h"
+
+namespace bldm {
+
+template <typename T, int VEC> struct VecIO {
+    __device__ __forceinline__ static void load(const T* p, T (&v)[VEC]) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) v[e] = p[e];
+    }
+    __device__ __forceinline__ static void store(T* p, const T (&v)[VEC]) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) __stcs(p + e, v[e]);
+    }
+};
+template <> struct VecIO<double, 2> {
+    __device__ __forceinline__ static void load(const double* p, double (&v)[2]) {
+        const double2 t = *reinterpret_cast<const double2*>(p);
+        v[0] = t.x;
+        v[1] = t.y;
+    }
+    __device__ __forceinline__ static void store(double* p, const double (&v)[2]) {
+        __stcs(reinterpret_cast<double2*>(p), make_double2(v[0], v[1]));
+    }
+};
+template <> struct VecIO<float, 4> {
+    __device__ __forceinline__ static void load(const float* p, float (&v)[4]) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    }
+    __device__ __forceinline__ static void store(float* p, const float (&v)[4]) {
+        __stcs(reinterpret_cast<float4*>(p), make_float4(v[0], v[1], v[2], v[3]));
+    }
+};
+
+__device__ __forceinline__ uintptr_t align_down16(uintptr_t a) { return a & ~uintptr_t(15); }
+__device__ __forceinline__ uintptr_t align_up16(uintptr_t a) {
+    return (a + 15) & ~uintptr_t(15);
+}
+
+// The sweep over one tile (band, row range) of one instance.  Lane layout:
+// lane = g*LPF + q handles fiber slot g of its warp and elements
+// k = (m*LPF + q)*VEC + v; warp w works on row slot w / wpr and column group
+// w % wpr of the band.
+template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool BATCH, bool MULTIROW>
+__device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLaunch& L, int band,
+                                           int rr, int tile, unsigned char* smem) {
+    constexpr int NW = kSweepWarps;
+    constexpr int FPW = 32 / LPF;
+    constexpr int CPW = cpw_for(MCH * VEC * int(sizeof(T)));
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int g = lane / LPF;
+    const int q = lane % LPF;
+    // MULTIROW == false: one row per stage (wpr == NW), the common wide-row case
+    // compiled without the row-slot arithmetic.
+    const int wpr = MULTIROW ? in.wpr : NW;
+    const int RPS = MULTIROW ? NW / wpr : 1;
+    const int rs = MULTIROW ? warp / wpr : 0;      // row slot of this warp
+    const int cg = MULTIROW ? warp % wpr : warp;   // column group of this warp
+
+    const long long z = in.z;
+    const long long c0 = (long long)band * in.band_w;
+    const int cw = (int)min((long long)in.band_w, in.y - c0);
+    const long long r0 = (long long)rr * in.rr_base + min(rr, in.rr_extra);
+    const int nrows = (int)min((long long)(in.rr_base + (rr < in.rr_extra ? 1 : 0)), in.x - r0);
+    const int nrounds = (nrows + RPS - 1) / RPS;
+    const SlotLayout lay(in.band_w, z, int(sizeof(T)));
+
+    unsigned char* stage0 = smem;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)L.stages * L.stage_bytes);
+    double* red = reinterpret_cast<double*>(bars + 8);                    // [stages][NW][z]
+    T* sAS = reinterpret_cast<T*>(red + (size_t)L.stages * NW * z);         // [z]
+    __shared__ int cnt[8];             // per-stage arrivals of warps (monotonic)
+    __shared__ double2 ltab[kLogTabN];  // ln table of the FP64 digamma
+    __shared__ double dsum[NW][2];
+
+    if (tid == 0) {
+        for (int s = 0; s < L.stages; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    if (tid < 8) cnt[tid] = 0;
+    if (UPDATE) {
+        for (long long k = tid; k < z; k += kSweepThreads) sAS[k] = in.psiAS[k];
+        if (sizeof(T) == 8 && APPR) log_tab_init(ltab, tid, kSweepThreads);
+    }
+    __syncthreads();
+
+    const uint64_t pol_stream = policy_evict_first();
+    const uint64_t pol_keep = policy_evict_last();
+
+    auto slotS = [&](unsigned char* st, int r) { return st + (size_t)r * lay.capS; };
+    auto slotX = [&](unsigned char* st, int r) {
+        return st + (size_t)RPS * lay.capS + (size_t)r * lay.capX;
+    };
+    auto slotA = [&](unsigned char* st, int r) {
+        return st + (size_t)RPS * (lay.capS + lay.capX) + (size_t)r * lay.capA;
+    };
+
+    // Round t holds rows r0 + t*RPS + r, r < RPS.
+    auto issue = [&](int t) {
+        const int s = t % L.stages;
+        unsigned char* st = stage0 + (size_t)s * L.stage_bytes;
+        const int nr = min(RPS, nrows - t * RPS);
+        uint32_t tot = 0;
+        for (int r = 0; r < nr; ++r) {
+            const long long i = r0 + (long long)t * RPS + r;
+            const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
+            const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
+            tot += uint32_t(align_up16(aS + (uintptr_t)cw * z * sizeof(T)) - align_down16(aS));
+            tot += uint32_t(align_up16(aX + (uintptr_t)cw * sizeof(T)) - align_down16(aX));
+            if (UPDATE) {
+                const uintptr_t aA = reinterpret_cast<uintptr_t>(in.psiA + i * z);
+                tot += uint32_t(align_up16(aA + (uintptr_t)z * sizeof(T)) - align_down16(aA));
+            }
+        }
+        mbar_arrive_expect_tx(&bars[s], tot);
+        for (int r = 0; r < nr; ++r) {
+            const long long i = r0 + (long long)t * RPS + r;
+            const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
+            const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
+            bulk_g2s(slotS(st, r), reinterpret_cast<const void*>(align_down16(aS)),
+                     uint32_t(align_up16(aS + (uintptr_t)cw * z * sizeof(T)) - align_down16(aS)),
+                     &bars[s], pol_stream);
+            bulk_g2s(slotX(st, r), reinterpret_cast<const void*>(align_down16(aX)),
+                     uint32_t(align_up16(aX + (uintptr_t)cw * sizeof(T)) - align_down16(aX)),
+                     &bars[s], pol_keep);
+            if (UPDATE) {
+                const uintptr_t aA = reinterpret_cast<uintptr_t>(in.psiA + i * z);
+                bulk_g2s(slotA(st, r), reinterpret_cast<const void*>(align_down16(aA)),
+                         uint32_t(align_up16(aA + (uintptr_t)z * sizeof(T)) - align_down16(aA)),
+                         &bars[s], pol_keep);
+            }
+        }
+    };
+
+    if (tid == 0) {
+        const int n0 = min(L.stages, nrounds);
+        for (int t = 0; t < n0; ++t) issue(t);
+    }
+
+    // Per-lane constants for the band: psi(beta_eph) of the lane's fibers.
+    T pB[CPW][MCH][VEC];
+    Acc<T> pj[CPW][MCH][VEC];
+#pragma unroll
+    for (int c = 0; c < CPW; ++c) {
+        const int jl = (cg * CPW + c) * FPW + g;
+#pragma unroll
+        for (int m = 0; m < MCH; ++m) {
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) {
+                const long long k = (long long)(m * LPF + q) * VEC + v;
+                pj[c][m][v].init();
+                if (UPDATE)
+                    pB[c][m][v] = (jl < cw && k < z) ? in.psiB[(c0 + jl) * z + k] : T(0);
+            }
+        }
+    }
+    // only multi-instance sweeps track the relative change
+    const bool track = BATCH && UPDATE && in.delta_part != nullptr;
+    double d_abs = 0.0, d_new = 0.0;
+
+    for (int t = 0; t < nrounds; ++t) {
+        const int s = t % L.stages;
+        // warp-uniform: the lane-group shuffles below need every lane of the warp
+        const bool ok =
+            __all_sync(0xffffffffu, mbar_wait_bounded(&bars[s], (uint32_t)((t / L.stages) & 1)));
+        if (!ok) {
+            // Give up: flag the error and wait (bounded) for the copies that
+            // may still be landing in this CTA's shared memory.
+            if (lane == 0) {
+                atomicOr(L.err, DEV_ERR_WAIT_TIMEOUT);
+                const int issued = min(nrounds, t + L.stages);
+                for (int u = t; u < issued; ++u)
+                    (void)mbar_wait_bounded(&bars[u % L.stages], (uint32_t)((u / L.stages) & 1));
+            }
+            return;
+        }
+        unsigned char* st = stage0 + (size_t)s * L.stage_bytes;
+        const bool row_ok = t * RPS + rs < nrows;  // warp-uniform
+        const long long i = r0 + (long long)t * RPS + rs;
+
+        Acc<T> ip[MCH][VEC];
+#pragma unroll
+        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) ip[m][v].init();
+
+        if (row_ok) {
+            const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
+            const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
+            const T* sS = reinterpret_cast<const T*>(slotS(st, rs) + (aS & 15));
+            const T* sX = reinterpret_cast<const T*>(slotX(st, rs) + (aX & 15));
+            T gm[MCH][VEC];
+            if (UPDATE) {
+                const uintptr_t aA = reinterpret_cast<uintptr_t>(in.psiA + i * z);
+                const T* sA = reinterpret_cast<const T*>(slotA(st, rs) + (aA & 15));
+#pragma unroll
+                for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                    for (int v = 0; v < VEC; ++v) {
+                        const long long k = (long long)(m * LPF + q) * VEC + v;
+                        gm[m][v] = (k < z) ? sAS[k] - sA[k] : T(0);
+                    }
+            }
+            T sv[CPW][MCH][VEC];
+            T xv[CPW];
+#pragma unroll
+            for (int c = 0; c < CPW; ++c) {
+                const int jl = (cg * CPW + c) * FPW + g;
+                const bool fv = jl < cw;
+#pragma unroll
+                for (int m = 0; m < MCH; ++m) {
+                    const long long k0 = (long long)(m * LPF + q) * VEC;
+                    // VEC > 1 only when z*sizeof(T) is a multiple of 16, so a
+                    // chunk is entirely inside or entirely outside the fiber.
+                    if (fv && k0 < z) {
+                        VecIO<T, VEC>::load(sS + (long long)jl * z + k0, sv[c][m]);
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < VEC; ++v) sv[c][m][v] = T(0);
+                    }
+                }
+                xv[c] = (UPDATE && fv) ? sX[jl] : T(0);
+            }
+            if (UPDATE) {
+                const T teps = T(L.eps);
+#pragma unroll
+                for (int c = 0; c < CPW; ++c) {
+                    const int jl = (cg * CPW + c) * FPW + g;
+                    const bool fv = jl < cw;
+                    T sn[MCH][VEC];
+                    // A fiber with X == 0 updates to zero whatever its digamma
+                    // values (the reference formula multiplies by X/(S_ijp+eps));
+                    // a pass whose fibers all have X == 0 skips the arithmetic.
+                    if (__any_sync(0xffffffffu, xv[c] != T(0))) {
+                        T arg[MCH * VEC], ps[MCH * VEC];
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) arg[m * VEC + v] = sv[c][m][v] + T(1);
+                        PsiPass<T, APPR>::template run<MCH * VEC>(arg, ps, ltab);
+                        T gp[MCH][VEC];
+                        T as = T(0), an = T(0), ad = T(0);
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) {
+                                const T e = sv[c][m][v];
+                                gp[m][v] = pB[c][m][v] - ps[m * VEC + v];
+                                as += e;
+                                an += e * gm[m][v];
+                                ad += e * gp[m][v];
+                            }
+                        as = group_sum<LPF>(as);
+                        an = group_sum<LPF>(an);
+                        ad = group_sum<LPF>(ad);
+                        const T xr = T(1) / (xv[c] + teps);
+                        const T nom = an * xr;
+                        const T den = ad * xr + teps;
+                        const T xos = xv[c] / (as + teps);
+                        // X == 0 (or an all-zero fiber) keeps the fiber at zero: the
+                        // reference's FP64 result, and no 0 * inf in FP32 where
+                        // eps = 1e-50 underflows to zero.
+                        const bool zero = (xv[c] == T(0)) || (as == T(0));
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v)
+                                sn[m][v] = zero ? T(0)
+                                                : sv[c][m][v] * (((gp[m][v] + nom) * xos) *
+                                                                 Rcp<T>::of(gm[m][v] + den));
+                    } else {
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) sn[m][v] = T(0);
+                    }
+#pragma unroll
+                    for (int m = 0; m < MCH; ++m) {
+#pragma unroll
+                        for (int v = 0; v < VEC; ++v) {
+                            pj[c][m][v].add(sn[m][v]);
+                            ip[m][v].add(sn[m][v]);
+                            if (track) {
+                                d_abs += fabs(double(sn[m][v]) - double(sv[c][m][v]));
+                                d_new += fabs(double(sn[m][v]));
+                            }
+                        }
+                        const long long k0 = (long long)(m * LPF + q) * VEC;
+                        if (fv && k0 < z)
+                            VecIO<T, VEC>::store(in.S + ((i * in.y + c0 + jl) * z + k0), sn[m]);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < CPW; ++c)
+#pragma unroll
+                    for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                        for (int v = 0; v < VEC; ++v) {
+                            pj[c][m][v].add(sv[c][m][v]);
+                            ip[m][v].add(sv[c][m][v]);
+                        }
+            }
+        }
+
+        // S_ipk partial of row i over this warp's columns -> red[s][warp].
+        double* redw = red + ((size_t)s * NW + warp) * z;
+#pragma unroll
+        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) {
+                double val = ip[m][v].value();
+                if (FPW > 1) val = cross_group_sum<LPF>(val);
+                const long long k = (long long)(m * LPF + q) * VEC + v;
+                if (g == 0 && k < z) redw[k] = val;
+            }
+        __syncwarp();
+        // No CTA barrier per round: each warp counts itself done with stage s;
+        // the last of the NW warps (the count reaches a multiple of NW) adds, per
+        // row slot, its warps' partials in column-group order, writes the S_ipk
+        // partials of the round's rows and refills the stage.  Warps drift apart
+        // by up to `stages` rounds.
+        int last = 0;
+        if (lane == 0) {
+            __threadfence_block();
+            last = (atomicAdd(&cnt[s], 1) == (t / L.stages + 1) * NW - 1) ? 1 : 0;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last) {
+            __threadfence_block();
+            const double* reds = red + (size_t)s * NW * z;
+            const int nr = min(RPS, nrows - t * RPS);
+            for (int r = 0; r < nr; ++r) {
+                const long long ir = r0 + (long long)t * RPS + r;
+                const double* redr = reds + (size_t)r * wpr * z;
+                for (long long k = lane; k < z; k += 32) {
+                    // all loads issued together; warps beyond wpr add nothing
+                    double part[NW];
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) part[w] = w < wpr ? redr[(size_t)w * z + k] : 0.0;
+                    double sum = 0.0;
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) sum += part[w];
+                    in.part_ipk[((long long)band * in.x + ir) * z + k] = sum;
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && t + L.stages < nrounds) issue(t + L.stages);
+        }
+    }
+
+    // S_pjk partial of the band over this tile's rows.  With one row slot every
+    // (j,k) has a single owner lane; otherwise the row slots' partials are added
+    // in slot order through shared memory (the drained stage ring).
+    if (RPS == 1) {
+#pragma unroll
+        for (int c = 0; c < CPW; ++c) {
+            const int jl = (cg * CPW + c) * FPW + g;
+#pragma unroll
+            for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                for (int v = 0; v < VEC; ++v) {
+                    const long long k = (long long)(m * LPF + q) * VEC + v;
+                    if (jl < cw && k < z)
+                        in.part_pjk[((long long)rr * in.y + c0 + jl) * z + k] = pj[c][m][v].value();
+                }
+        }
+    } else {
+        __syncthreads();  // every warp is done with the ring
+        double* pjbuf = reinterpret_cast<double*>(stage0);  // [RPS][band_w][z]
+#pragma unroll
+        for (int c = 0; c < CPW; ++c) {
+            const int jl = (cg * CPW + c) * FPW + g;
+#pragma unroll
+            for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                for (int v = 0; v < VEC; ++v) {
+                    const long long k = (long long)(m * LPF + q) * VEC + v;
+                    if (jl < in.band_w && k < z)
+                        pjbuf[((size_t)rs * in.band_w + jl) * z + k] = pj[c][m][v].value();
+                }
+        }
+        __syncthreads();
+        const long long n = (long long)cw * z;
+        for (long long e = tid; e < n; e += kSweepThreads) {
+            double sum = 0.0;
+            for (int r = 0; r < RPS; ++r) sum += pjbuf[(size_t)r * in.band_w * z + e];
+            in.part_pjk[((long long)rr * in.y + c0) * z + e] = sum;
+        }
+    }
+
+    if (track) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d_abs += __shfl_xor_sync(0xffffffffu, d_abs, o);
+            d_new += __shfl_xor_sync(0xffffffffu, d_new, o);
+        }
+        if (lane == 0) {
+            dsum[warp][0] = d_abs;
+            dsum[warp][1] = d_new;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double a = 0.0, b = 0.0;
+            for (int w = 0; w < NW; ++w) {
+                a += dsum[w][0];
+                b += dsum[w][1];
+            }
+            in.delta_part[2 * tile] = a;
+            in.delta_part[2 * tile + 1] = b;
+        }
+    }
+}
+
+template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool MULTIROW>
+__global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepParams<T> p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int band = blockIdx.x % p.in.n_bands;
+    const int rr = blockIdx.x / p.in.n_bands;
+    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR, false, MULTIROW>(p.in, p.L, band, rr,
+                                                               int(blockIdx.x), smem);
+}
+
+template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool MULTIROW>
+__global__ void __launch_bounds__(kSweepThreads, 2) sweep_batch_kernel(const BatchSweepParams<T> p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const BatchTile tl = p.tiles[blockIdx.x];
+    SweepInst<T> in = p.insts[tl.inst];
+    if (!p.track) in.delta_part = nullptr;
+    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR, true, MULTIROW>(in, p.L, tl.band, tl.rr,
+                                                              tl.rr * in.n_bands + tl.band, smem);
+}
+
+
+}  // namespace bldm
