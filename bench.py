@@ -501,6 +501,68 @@ def run_serve(args):
     return 0
 
 
+def run_precision(args):
+    """FP32 storage with compensated axis sums against the FP64 path."""
+    import torch
+    pkg = load_package()
+    import bnmf_algs_b200.workloads as W
+    base = W.precision_study(2)
+    X, z = base["X"], base["z"]
+    x, y = X.shape
+    # as specified, and the same draws mapped onto U(1,2) (grad_plus >= 0 there)
+    variants = [("alpha,beta~U(0.5,2)", base["alpha"], base["beta"]),
+                ("alpha,beta~U(1,2)", 1.0 + (base["alpha"] - 0.5) / 1.5,
+                 1.0 + (base["beta"] - 0.5) / 1.5)]
+    out = []
+    for name, alpha, beta in variants:
+        params = pkg.Params(base["a"], base["b"], alpha, beta)
+        da = torch.as_tensor(alpha).cuda()
+        db = torch.as_tensor(beta).cuda()
+        dX64 = torch.as_tensor(X).cuda()
+        dX32 = dX64.float()
+        p64 = pkg.Plan(x, y, z, pkg.F64)
+        p32 = pkg.Plan(x, y, z, pkg.F32)
+        S64 = torch.empty((x, y, z), dtype=torch.float64, device="cuda")
+        p64.init_S(dX64, S64, seed=0)
+        S32 = S64.float()
+        Xf = dX64.unsqueeze(2)
+        rows = []
+        done = 0
+        for ck in range(25, base["iters"] + 1, 25):
+            p64.run(dX64, da, db, S64, ck - done, pkg.PSI_APPR)
+            p32.run(dX32, da, db, S32, ck - done, pkg.PSI_APPR)
+            p64.check()
+            p32.check()
+            done = ck
+            finite64 = bool(torch.isfinite(S64).all())
+            finite32 = bool(torch.isfinite(S32).all())
+            row = {"iteration": ck, "fp64_finite": finite64, "fp32_finite": finite32,
+                   "fp64_negative": int((S64 < 0).sum())}
+            if finite64 and finite32:
+                mask = S64 > 1e-6 * Xf
+                rel = ((S32.double() - S64).abs() / S64.abs().clamp_min(1e-300))[mask]
+                row["max_rel_err_S"] = float(rel.max()) if rel.numel() else 0.0
+                row["median_rel_err_S"] = float(rel.median()) if rel.numel() else 0.0
+                den = dX64.clamp_min(1.0)
+                row["conservation_fp64"] = float(((S64.sum(2) - dX64).abs() / den).max())
+                row["conservation_fp32"] = float(((S32.double().sum(2) - dX64).abs() / den).max())
+                lm64 = pkg.log_marginal_S(S64, params)
+                lm32 = pkg.log_marginal_S(S32, params, dtype=pkg.F32)
+                row["log_marginal_fp64"] = lm64
+                row["log_marginal_gap_rel"] = abs(lm32 - lm64) / abs(lm64)
+            rows.append(row)
+        out.append({"params": name, "checkpoints": rows})
+        p64.close()
+        p32.close()
+    line = {"metric": "precision_fp32_vs_fp64", "dtype": "f32 vs f64", "data": "synthetic",
+            "config": {"workload": "precision_2048x2048x32", "iters": base["iters"],
+                       "X": "Poisson(rate_i), rate_i~LogNormal(0,1.5), 30% zeros",
+                       "zero_fraction": float(np.mean(X == 0))},
+            "results": out}
+    print(json.dumps(line))
+    return 0
+
+
 def make_X(kind, x, y, z, rng):
     """X kinds: 'model' (the plain workload's allocation-model draw), 'dense'
     (1 + Poisson(10), no zeros), 'zeros' (all zero)."""
@@ -577,10 +639,17 @@ def main():
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--duration", type=float, default=20.0)
     ap.add_argument("--fp64-sample", type=int, default=16)
+    ap.add_argument("--precision", action="store_true",
+                    help="precision study: 2048x2048x32 heavy-tailed X, FP32 (compensated sums) "
+                         "vs the FP64 path, 300 iterations, checkpoints every 25")
     ap.add_argument("--kernel-matrix", action="store_true",
                     help="time the update sweep (CUDA events) over X kinds, dtypes and launch "
                          "knobs; one JSON line each")
     args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.dtype is None:
+        args.dtype = "f32" if (args.batch or args.serve) else "f64"
     if args.profile_run:
         return run_profile(args)
     if args.kernel_matrix:
@@ -589,10 +658,8 @@ def main():
         return run_batch(args)
     if args.serve:
         return run_serve(args)
-    if args.warmup < 3:
-        args.warmup = 3
-    if args.dtype is None:
-        args.dtype = "f32" if (args.batch or args.serve) else "f64"
+    if args.precision:
+        return run_precision(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
