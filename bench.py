@@ -327,7 +327,10 @@ def run_profile(args):
     import bnmf_algs_b200.workloads as W
     x, y, z = (int(v) for v in args.shape.split("x"))
     rng = np.random.default_rng(1)
-    X = W.allocation_model_X(x, y, z, 5.0, 0.01 if x * y >= 1 << 20 else 0.1, rng)
+    if args.x_kind == "model":
+        X = W.allocation_model_X(x, y, z, 5.0, 0.01 if x * y >= 1 << 20 else 0.1, rng)
+    else:
+        X = make_X(args.x_kind, x, y, z, rng)
     f64 = args.dtype == "f64"
     dt_t = torch.float64 if f64 else torch.float32
     dX = torch.as_tensor(X).to("cuda", dt_t)
@@ -626,6 +629,8 @@ def main():
                     help="untimed: set up the workload, run --profile-iters iterations, exit "
                          "(the command profiled by ncu)")
     ap.add_argument("--profile-iters", type=int, default=3)
+    ap.add_argument("--x-kind", choices=["model", "dense", "zeros"], default="model",
+                    help="X of --profile-run: the plain workload's draw, 1+Poisson(10), or zeros")
     ap.add_argument("--shape", default="1024x1024x64",
                     help="x*y*z of the plain workload for --profile-run / --kernel-matrix")
     ap.add_argument("--batch", action="store_true",

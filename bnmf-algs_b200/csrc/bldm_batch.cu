@@ -74,6 +74,10 @@ int bldm_batch_create(bldm_batch** out, int dtype, size_t n, const size_t* xs, c
         b->eng->bind(b->inst[i], static_cast<char*>(b->arena) + off[i]);
         ptrs[i] = &b->inst[i];
     }
+    for (size_t i = 0; i < n; ++i) {
+        e = cudaMemset(b->inst[i].counter, 0, 16);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
     int rc = b->eng->build(ptrs, nullptr);
     if (rc) return rc;
     rc = cuda_status(cudaDeviceSynchronize());

@@ -124,13 +124,12 @@ void Engine::bind(EngineInstance& in, void* base) const {
 }
 
 void Engine::free_tables() {
-    for (auto& c : classes_) {
-        if (c.d_tiles) cudaFree(c.d_tiles);
-        c.d_tiles = nullptr;
-    }
+    for (auto& c : classes_) c.d_tiles = nullptr;
     if (d_tables_) cudaFree(d_tables_);
+    if (h_stage_) cudaFreeHost(h_stage_);
     d_tables_ = nullptr;
-    table_bytes_ = 0;
+    h_stage_ = nullptr;
+    table_bytes_ = table_cap_ = h_cap_ = 0;
 }
 
 void Engine::drop_graphs() {
@@ -190,7 +189,9 @@ static void fill_tables(const std::vector<EngineInstance*>& insts, std::vector<c
 
 int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
     drop_graphs();
-    free_tables();
+    // The previous tables may still be read by work queued on st; the new ones
+    // are written on st behind it, so the device buffer can be reused.
+    for (auto& c : classes_) c.d_tiles = nullptr;
     insts_ = insts;
     // Lane-shape classes, keeping streams of classes that already exist.
     std::vector<ShapeClass> old;
@@ -258,7 +259,7 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
         for (int rr = 0; rr < c.n_rr; ++rr)
             for (int b = 0; b < c.n_bands; ++b) k.tiles.push_back(BatchTile{int(n), b, rr, 0});
     }
-    // Device tables: SweepInst[n] | FinInst[n] | block_off[n+1] | err.
+    // Device tables: SweepInst[n] | FinInst[n] | block_off[n+1] | err | tiles per class.
     const size_t n = insts.size();
     const size_t s_sz = dtype_ == BLDM_F64 ? sizeof(SweepInst<double>) : sizeof(SweepInst<float>);
     const size_t f_sz = dtype_ == BLDM_F64 ? sizeof(FinInst<double>) : sizeof(FinInst<float>);
@@ -266,33 +267,59 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
     const size_t o_finst = a256(o_sinst + n * s_sz);
     const size_t o_boff = a256(o_finst + n * f_sz);
     const size_t o_err = a256(o_boff + (n + 1) * sizeof(int));
-    table_bytes_ = a256(o_err + 64);
-    std::vector<char> host(table_bytes_, 0);
+    size_t off = a256(o_err + 64);
+    std::vector<size_t> o_tiles(classes_.size());
+    for (size_t c = 0; c < classes_.size(); ++c) {
+        o_tiles[c] = off;
+        off = a256(off + classes_[c].tiles.size() * sizeof(BatchTile));
+    }
+    table_bytes_ = off;
+    if (table_bytes_ > h_cap_) {
+        // a pinned staging buffer may still feed an earlier async copy
+        ENG_CU(cudaStreamSynchronize(st));
+        if (h_stage_) cudaFreeHost(h_stage_);
+        h_stage_ = nullptr;
+        h_cap_ = 0;
+        ENG_CU(cudaMallocHost(&h_stage_, table_bytes_ * 2));
+        h_cap_ = table_bytes_ * 2;
+    } else {
+        ENG_CU(cudaStreamSynchronize(st));  // the staging buffer is free again
+    }
+    if (table_bytes_ > table_cap_) {
+        if (d_tables_) cudaFree(d_tables_);
+        d_tables_ = nullptr;
+        table_cap_ = 0;
+        ENG_CU(cudaMalloc(&d_tables_, table_bytes_ * 2));
+        table_cap_ = table_bytes_ * 2;
+    }
+    char* host = static_cast<char*>(h_stage_);
+    std::memset(host, 0, table_bytes_);
+    std::vector<char> hv;  // fill_tables works on a vector view of the staging buffer
+    hv.resize(o_boff);
     if (dtype_ == BLDM_F64)
-        fill_tables<double>(insts, host, o_sinst, o_finst);
+        fill_tables<double>(insts, hv, o_sinst, o_finst);
     else
-        fill_tables<float>(insts, host, o_sinst, o_finst);
-    int* boff = reinterpret_cast<int*>(host.data() + o_boff);
+        fill_tables<float>(insts, hv, o_sinst, o_finst);
+    std::memcpy(host, hv.data(), o_boff);
+    int* boff = reinterpret_cast<int*>(host + o_boff);
     fin_blocks_ = 0;
     for (size_t i = 0; i < n; ++i) {
         boff[i] = fin_blocks_;
         fin_blocks_ += insts[i]->nbB + insts[i]->cfg.n_ablk;
     }
     boff[n] = fin_blocks_;
-    ENG_CU(cudaMalloc(&d_tables_, table_bytes_));
     char* base = static_cast<char*>(d_tables_);
+    for (size_t c = 0; c < classes_.size(); ++c) {
+        std::memcpy(host + o_tiles[c], classes_[c].tiles.data(),
+                    classes_[c].tiles.size() * sizeof(BatchTile));
+        classes_[c].d_tiles = reinterpret_cast<BatchTile*>(base + o_tiles[c]);
+    }
     d_sinst_ = base + o_sinst;
     d_finst_ = base + o_finst;
     d_block_off_ = reinterpret_cast<int*>(base + o_boff);
     d_err_ = reinterpret_cast<int*>(base + o_err);
-    ENG_CU(cudaMemcpy(d_tables_, host.data(), table_bytes_, cudaMemcpyHostToDevice));
-    for (auto& k : classes_) {
-        ENG_CU(cudaMalloc(&k.d_tiles, k.tiles.size() * sizeof(BatchTile)));
-        ENG_CU(cudaMemcpy(k.d_tiles, k.tiles.data(), k.tiles.size() * sizeof(BatchTile),
-                          cudaMemcpyHostToDevice));
-        table_bytes_ += k.tiles.size() * sizeof(BatchTile);
-    }
-    for (EngineInstance* in : insts) ENG_CU(cudaMemsetAsync(in->counter, 0, 16, st));
+    ENG_CU(cudaMemcpyAsync(d_tables_, host, table_bytes_, cudaMemcpyHostToDevice, st));
+    (void)st;
     return BLDM_OK;
 }
 

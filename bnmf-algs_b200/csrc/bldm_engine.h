@@ -101,8 +101,11 @@ class Engine {
     int num_sms_;
     std::vector<EngineInstance*> insts_;
     std::vector<ShapeClass> classes_;
-    void* d_tables_ = nullptr;  // SweepInst[n] | FinInst[n] | block_off[n+1] | err
-    size_t table_bytes_ = 0;
+    void* d_tables_ = nullptr;  // SweepInst[n] | FinInst[n] | block_off[n+1] | err | tiles
+    size_t table_bytes_ = 0;    // bytes in use
+    size_t table_cap_ = 0;      // bytes allocated (grow-only across builds)
+    void* h_stage_ = nullptr;   // pinned host staging of the tables
+    size_t h_cap_ = 0;
     void* d_sinst_ = nullptr;
     void* d_finst_ = nullptr;
     int* d_block_off_ = nullptr;

@@ -97,6 +97,8 @@ int bldm_server::admit(Request* r) {
     }
     eng->bind(r->inst, r->dmem);
     r->inst.rel = d_rel + r->slot;
+    e = cudaMemsetAsync(r->inst.counter, 0, 16, stream);
+    if (e != cudaSuccess) return cuda_status(e);
     const size_t es = eng->es();
     if (es == 8) {
         e = cudaMemcpyAsync(r->inst.X, r->X.data(), r->x * r->y * 8, cudaMemcpyHostToDevice,

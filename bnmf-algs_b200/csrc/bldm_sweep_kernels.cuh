@@ -45,67 +45,6 @@ __device__ __forceinline__ uintptr_t align_up16(uintptr_t a) {
     return (a + 15) & ~uintptr_t(15);
 }
 
-// The update of NP passes of a warp (each lane: MCH*VEC elements of one fiber
-// per pass): digamma of S+1, grad_plus, the fiber sums S_ijp, nom and denom
-// (lane-group shuffles), and the new fiber values (update_S).
-template <int NP, int LPF, int MCH, int VEC, bool APPR, typename T>
-__device__ __forceinline__ void update_passes(const T (*sv)[MCH][VEC], const T (*pB)[MCH][VEC],
-                                              const T (&gm)[MCH][VEC], const T* xv, T teps,
-                                              const double2* ltab, T (*sn)[MCH][VEC]) {
-    constexpr int NE = NP * MCH * VEC;
-    T arg[NE], ps[NE];
-#pragma unroll
-    for (int p = 0; p < NP; ++p)
-#pragma unroll
-        for (int m = 0; m < MCH; ++m)
-#pragma unroll
-            for (int v = 0; v < VEC; ++v) arg[(p * MCH + m) * VEC + v] = sv[p][m][v] + T(1);
-    PsiPass<T, APPR>::template run<NE>(arg, ps, ltab);
-    T gp[NP][MCH][VEC];
-    T as[NP], an[NP], ad[NP];
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        as[p] = T(0);
-        an[p] = T(0);
-        ad[p] = T(0);
-#pragma unroll
-        for (int m = 0; m < MCH; ++m)
-#pragma unroll
-            for (int v = 0; v < VEC; ++v) {
-                const T e = sv[p][m][v];
-                gp[p][m][v] = pB[p][m][v] - ps[(p * MCH + m) * VEC + v];
-                as[p] += e;
-                an[p] += e * gm[m][v];
-                ad[p] += e * gp[p][m][v];
-            }
-    }
-#pragma unroll
-    for (int o = LPF / 2; o > 0; o >>= 1)
-#pragma unroll
-        for (int p = 0; p < NP; ++p) {
-            as[p] += __shfl_xor_sync(0xffffffffu, as[p], o);
-            an[p] += __shfl_xor_sync(0xffffffffu, an[p], o);
-            ad[p] += __shfl_xor_sync(0xffffffffu, ad[p], o);
-        }
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        const T xr = T(1) / (xv[p] + teps);
-        const T nom = an[p] * xr;
-        const T den = ad[p] * xr + teps;
-        const T xos = xv[p] / (as[p] + teps);
-        // X == 0 (or an all-zero fiber) keeps the fiber at zero: the reference's
-        // FP64 result, and no 0 * inf in FP32 where eps = 1e-50 underflows to zero.
-        const bool zero = (xv[p] == T(0)) || (as[p] == T(0));
-#pragma unroll
-        for (int m = 0; m < MCH; ++m)
-#pragma unroll
-            for (int v = 0; v < VEC; ++v)
-                sn[p][m][v] = zero ? T(0)
-                                   : sv[p][m][v] *
-                                         (((gp[p][m][v] + nom) * xos) * Rcp<T>::of(gm[m][v] + den));
-    }
-}
-
 // The sweep over one tile (band, row range) of one instance.  Lane layout:
 // lane = g*LPF + q handles fiber slot g of its warp and elements
 // k = (m*LPF + q)*VEC + v; warp w works on row slot w / wpr and column group
@@ -295,54 +234,71 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             }
             if (UPDATE) {
                 const T teps = T(L.eps);
-                T sn[CPW][MCH][VEC];
-                // A fiber with X == 0 updates to zero whatever its digamma values
-                // (the reference formula multiplies by X/(S_ijp+eps)); a pass whose
-                // fibers all have X == 0 skips the arithmetic.  When every pass of
-                // the row has work, the passes are evaluated as one batch, which
-                // gives the digamma and the reductions CPW times more independent
-                // instructions.
-                bool act[CPW];
-                int n_act = 0;
-#pragma unroll
-                for (int c = 0; c < CPW; ++c) {
-                    act[c] = __any_sync(0xffffffffu, xv[c] != T(0));
-                    n_act += act[c] ? 1 : 0;
-                }
-                if (CPW > 1 && n_act == CPW) {
-                    update_passes<CPW, LPF, MCH, VEC, APPR>(sv, pB, gm, xv, teps, ltab, sn);
-                } else {
-#pragma unroll
-                    for (int c = 0; c < CPW; ++c) {
-                        if (act[c]) {
-                            update_passes<1, LPF, MCH, VEC, APPR>(&sv[c], &pB[c], gm, &xv[c], teps,
-                                                                  ltab, &sn[c]);
-                        } else {
-#pragma unroll
-                            for (int m = 0; m < MCH; ++m)
-#pragma unroll
-                                for (int v = 0; v < VEC; ++v) sn[c][m][v] = T(0);
-                        }
-                    }
-                }
 #pragma unroll
                 for (int c = 0; c < CPW; ++c) {
                     const int jl = (cg * CPW + c) * FPW + g;
                     const bool fv = jl < cw;
+                    T sn[MCH][VEC];
+                    // A fiber with X == 0 updates to zero whatever its digamma
+                    // values (the reference formula multiplies by X/(S_ijp+eps));
+                    // a pass whose fibers all have X == 0 skips the arithmetic.
+                    if (__any_sync(0xffffffffu, xv[c] != T(0))) {
+                        T arg[MCH * VEC], ps[MCH * VEC];
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) arg[m * VEC + v] = sv[c][m][v] + T(1);
+                        PsiPass<T, APPR>::template run<MCH * VEC>(arg, ps, ltab);
+                        T gp[MCH][VEC];
+                        T as = T(0), an = T(0), ad = T(0);
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) {
+                                const T e = sv[c][m][v];
+                                gp[m][v] = pB[c][m][v] - ps[m * VEC + v];
+                                as += e;
+                                an += e * gm[m][v];
+                                ad += e * gp[m][v];
+                            }
+                        as = group_sum<LPF>(as);
+                        an = group_sum<LPF>(an);
+                        ad = group_sum<LPF>(ad);
+                        const T xr = T(1) / (xv[c] + teps);
+                        const T nom = an * xr;
+                        const T den = ad * xr + teps;
+                        const T xos = xv[c] / (as + teps);
+                        // X == 0 (or an all-zero fiber) keeps the fiber at zero: the
+                        // reference's FP64 result, and no 0 * inf in FP32 where
+                        // eps = 1e-50 underflows to zero.
+                        const bool zero = (xv[c] == T(0)) || (as == T(0));
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v)
+                                sn[m][v] = zero ? T(0)
+                                                : sv[c][m][v] * (((gp[m][v] + nom) * xos) *
+                                                                 Rcp<T>::of(gm[m][v] + den));
+                    } else {
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) sn[m][v] = T(0);
+                    }
 #pragma unroll
                     for (int m = 0; m < MCH; ++m) {
 #pragma unroll
                         for (int v = 0; v < VEC; ++v) {
-                            pj[c][m][v].add(sn[c][m][v]);
-                            ip[m][v].add(sn[c][m][v]);
+                            pj[c][m][v].add(sn[m][v]);
+                            ip[m][v].add(sn[m][v]);
                             if (track) {
-                                d_abs += fabs(double(sn[c][m][v]) - double(sv[c][m][v]));
-                                d_new += fabs(double(sn[c][m][v]));
+                                d_abs += fabs(double(sn[m][v]) - double(sv[c][m][v]));
+                                d_new += fabs(double(sn[m][v]));
                             }
                         }
                         const long long k0 = (long long)(m * LPF + q) * VEC;
                         if (fv && k0 < z)
-                            VecIO<T, VEC>::store(in.S + ((i * in.y + c0 + jl) * z + k0), sn[c][m]);
+                            VecIO<T, VEC>::store(in.S + ((i * in.y + c0 + jl) * z + k0), sn[m]);
                     }
                 }
             } else {
