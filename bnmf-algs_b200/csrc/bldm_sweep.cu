@@ -30,11 +30,36 @@
 
 namespace bldm {
 
+// Sum of p[r * stride], r < n, in increasing r (the order of a plain loop),
+// with the loads of eight terms issued before their adds so that a thread keeps
+// eight reads of the partial buffers in flight.
+template <bool CG>
+__device__ __forceinline__ double sum_strided(const double* p, long long stride, int n) {
+    double s = 0.0;
+    int r = 0;
+    for (; r + 8 <= n; r += 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const double* a = p + (long long)(r + u) * stride;
+            v[u] = CG ? __ldcg(a) : *a;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s += v[u];
+    }
+    for (; r < n; ++r) {
+        const double* a = p + (long long)r * stride;
+        s += CG ? __ldcg(a) : *a;
+    }
+    return s;
+}
+
 // Block `blk` of an instance's finalize.  Blocks [0, nbB): psi(beta_eph) for
 // every (j,k).  Blocks [nbB, nbB + n_ablk): psi(alpha_eph) for a block of rows
 // plus that block's sum of alpha_eph over rows; the last block to finish sums
-// the block sums in order, tabulates psi(sum_i alpha_eph(i,k)) and, when the
-// sweep tracked it, the relative change of S.
+// the block sums (R interleaved groups of blocks, then the groups in order),
+// tabulates psi(sum_i alpha_eph(i,k)) and, when the sweep tracked it, the
+// relative change of S.
 template <typename T>
 __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int plus_appr,
                                                int minus_appr) {
@@ -44,8 +69,7 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
         const long long idx = (long long)blk * kFinThreads + tid;
         if (idx < p.y * z) {
             const long long k = idx % z;
-            double s = 0.0;
-            for (int r = 0; r < p.n_rr; ++r) s += p.part_pjk[(long long)r * p.y * z + idx];
+            const double s = sum_strided<false>(p.part_pjk + idx, p.y * z, p.n_rr);
             p.psiB[idx] = T(psi_mode_f64(s + p.beta[k], plus_appr != 0));
         }
         return;
@@ -62,9 +86,7 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
         for (long long k = tid % KT; k < z; k += KT) {
             double a = 0.0;
             for (long long i = i0 + sub; i < i1; i += R) {
-                double s = 0.0;
-                for (int bd = 0; bd < p.n_bands; ++bd)
-                    s += p.part_ipk[((long long)bd * p.x + i) * z + k];
+                const double s = sum_strided<false>(p.part_ipk + i * z + k, p.x * z, p.n_bands);
                 const double ae = s + p.alpha[i];
                 p.psiA[i * z + k] = T(psi_mode_f64(ae, minus_appr != 0));
                 a += ae;
@@ -84,18 +106,33 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
     __syncthreads();
     if (last) {
         __threadfence();
+        // group r < R sums blocks r, r + R, r + 2R, ... of column k
+        if (sub < R) {
+            for (long long k = tid % KT; k < z; k += KT) {
+                const int nb = (p.n_ablk - sub + R - 1) / R;
+                acc[sub * z + k] =
+                    sum_strided<true>(p.asum_part + (long long)sub * z + k, (long long)R * z, nb);
+            }
+        }
+        __syncthreads();
         for (long long k = tid; k < z; k += kFinThreads) {
             double a = 0.0;
-            for (int bb = 0; bb < p.n_ablk; ++bb) a += __ldcg(&p.asum_part[(long long)bb * z + k]);
+            for (int r = 0; r < R; ++r) a += acc[r * z + k];
             p.psiAS[k] = T(psi_mode_f64(a, minus_appr != 0));
         }
-        if (p.delta_part && tid == 0) {
+        if (p.delta_part && tid < 32) {
+            // lanes take tiles t = lane, lane + 32, ...; then a fixed-order tree
             double d = 0.0, n = 0.0;
-            for (int t = 0; t < p.n_tiles; ++t) {
+            for (int t = tid; t < p.n_tiles; t += 32) {
                 d += __ldcg(&p.delta_part[2 * t]);
                 n += __ldcg(&p.delta_part[2 * t + 1]);
             }
-            *p.rel_change = n > 0.0 ? d / n : (d > 0.0 ? 1.0 : 0.0);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                d += __shfl_xor_sync(0xffffffffu, d, o);
+                n += __shfl_xor_sync(0xffffffffu, n, o);
+            }
+            if (tid == 0) *p.rel_change = n > 0.0 ? d / n : (d > 0.0 ? 1.0 : 0.0);
         }
         if (tid == 0) *p.counter = 0u;
     }

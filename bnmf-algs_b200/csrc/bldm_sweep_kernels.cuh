@@ -234,72 +234,133 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             }
             if (UPDATE) {
                 const T teps = T(L.eps);
+                // A fiber with X == 0 updates to zero whatever its digamma values
+                // (the reference formula multiplies by X/(S_ijp+eps)).  Passes
+                // whose fibers all have X == 0 only store zeros; the others form
+                // a warp-uniform work list that runs one copy of the arithmetic,
+                // gathering the pass's operands by selects.
+                unsigned work = 0;
 #pragma unroll
-                for (int c = 0; c < CPW; ++c) {
-                    const int jl = (cg * CPW + c) * FPW + g;
-                    const bool fv = jl < cw;
-                    T sn[MCH][VEC];
-                    // A fiber with X == 0 updates to zero whatever its digamma
-                    // values (the reference formula multiplies by X/(S_ijp+eps));
-                    // a pass whose fibers all have X == 0 skips the arithmetic.
-                    if (__any_sync(0xffffffffu, xv[c] != T(0))) {
-                        T arg[MCH * VEC], ps[MCH * VEC];
+                for (int c = 0; c < CPW; ++c)
+                    if (__any_sync(0xffffffffu, xv[c] != T(0))) work |= 1u << c;
+
+                // The update of one pass from its fiber values se, psi(beta_eph)
+                // values be and X value xe.
+                auto pass_math = [&](const T (&se)[MCH][VEC], const T (&be)[MCH][VEC], const T xe,
+                                     T (&sn)[MCH][VEC]) {
+                    // digamma in chunks of at most 4 elements per lane (bounds
+                    // the live registers of long fibers)
+                    constexpr int NE = MCH * VEC;
+                    constexpr int NC = NE < 4 ? NE : 4;
+                    T ps[NE];
 #pragma unroll
-                        for (int m = 0; m < MCH; ++m)
+                    for (int e0 = 0; e0 < NE; e0 += NC) {
+                        T arg[NC], out[NC];
 #pragma unroll
-                            for (int v = 0; v < VEC; ++v) arg[m * VEC + v] = sv[c][m][v] + T(1);
-                        PsiPass<T, APPR>::template run<MCH * VEC>(arg, ps, ltab);
-                        T gp[MCH][VEC];
-                        T as = T(0), an = T(0), ad = T(0);
+                        for (int e = 0; e < NC; ++e)
+                            arg[e] = se[(e0 + e) / VEC][(e0 + e) % VEC] + T(1);
+                        PsiPass<T, APPR>::template run<NC>(arg, out, ltab);
 #pragma unroll
-                        for (int m = 0; m < MCH; ++m)
-#pragma unroll
-                            for (int v = 0; v < VEC; ++v) {
-                                const T e = sv[c][m][v];
-                                gp[m][v] = pB[c][m][v] - ps[m * VEC + v];
-                                as += e;
-                                an += e * gm[m][v];
-                                ad += e * gp[m][v];
-                            }
-                        as = group_sum<LPF>(as);
-                        an = group_sum<LPF>(an);
-                        ad = group_sum<LPF>(ad);
-                        const T xr = T(1) / (xv[c] + teps);
-                        const T nom = an * xr;
-                        const T den = ad * xr + teps;
-                        const T xos = xv[c] / (as + teps);
-                        // X == 0 (or an all-zero fiber) keeps the fiber at zero: the
-                        // reference's FP64 result, and no 0 * inf in FP32 where
-                        // eps = 1e-50 underflows to zero.
-                        const bool zero = (xv[c] == T(0)) || (as == T(0));
-#pragma unroll
-                        for (int m = 0; m < MCH; ++m)
-#pragma unroll
-                            for (int v = 0; v < VEC; ++v)
-                                sn[m][v] = zero ? T(0)
-                                                : sv[c][m][v] * (((gp[m][v] + nom) * xos) *
-                                                                 Rcp<T>::of(gm[m][v] + den));
-                    } else {
-#pragma unroll
-                        for (int m = 0; m < MCH; ++m)
-#pragma unroll
-                            for (int v = 0; v < VEC; ++v) sn[m][v] = T(0);
+                        for (int e = 0; e < NC; ++e) ps[e0 + e] = out[e];
                     }
+                    T gp[MCH][VEC];
+                    T as = T(0), an = T(0), ad = T(0);
+#pragma unroll
+                    for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                        for (int v = 0; v < VEC; ++v) {
+                            const T e = se[m][v];
+                            gp[m][v] = be[m][v] - ps[m * VEC + v];
+                            as += e;
+                            an += e * gm[m][v];
+                            ad += e * gp[m][v];
+                        }
+                    as = group_sum<LPF>(as);
+                    an = group_sum<LPF>(an);
+                    ad = group_sum<LPF>(ad);
+                    const T xr = Rcp<T>::of(xe + teps);
+                    const T nom = an * xr;
+                    const T den = ad * xr + teps;
+                    const T xos = xe * Rcp<T>::of(as + teps);
+                    // X == 0 (or an all-zero fiber) keeps the fiber at zero: the
+                    // reference's FP64 result, and no 0 * inf in FP32 where
+                    // eps = 1e-50 underflows to zero.
+                    const bool zero = (xe == T(0)) || (as == T(0));
+#pragma unroll
+                    for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                        for (int v = 0; v < VEC; ++v)
+                            sn[m][v] = zero ? T(0)
+                                            : se[m][v] * (((gp[m][v] + nom) * xos) *
+                                                          Rcp<T>::of(gm[m][v] + den));
+                };
+                // Accumulates and stores the new values of pass c.
+                auto pass_out = [&](const int c, const T (&se)[MCH][VEC], const T (&sn)[MCH][VEC]) {
+                    const int jl = (cg * CPW + c) * FPW + g;
 #pragma unroll
                     for (int m = 0; m < MCH; ++m) {
 #pragma unroll
                         for (int v = 0; v < VEC; ++v) {
-                            pj[c][m][v].add(sn[m][v]);
                             ip[m][v].add(sn[m][v]);
                             if (track) {
-                                d_abs += fabs(double(sn[m][v]) - double(sv[c][m][v]));
+                                d_abs += fabs(double(sn[m][v]) - double(se[m][v]));
                                 d_new += fabs(double(sn[m][v]));
                             }
                         }
                         const long long k0 = (long long)(m * LPF + q) * VEC;
-                        if (fv && k0 < z)
+                        if (jl < cw && k0 < z)
                             VecIO<T, VEC>::store(in.S + ((i * in.y + c0 + jl) * z + k0), sn[m]);
                     }
+                };
+
+#pragma unroll
+                for (int c = 0; c < CPW; ++c) {
+                    if ((work >> c) & 1u) continue;
+                    const int jl = (cg * CPW + c) * FPW + g;
+                    T zs[VEC];
+#pragma unroll
+                    for (int v = 0; v < VEC; ++v) zs[v] = T(0);
+#pragma unroll
+                    for (int m = 0; m < MCH; ++m) {
+                        if (track) {
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) d_abs += fabs(double(sv[c][m][v]));
+                        }
+                        const long long k0 = (long long)(m * LPF + q) * VEC;
+                        if (jl < cw && k0 < z)
+                            VecIO<T, VEC>::store(in.S + ((i * in.y + c0 + jl) * z + k0), zs);
+                    }
+                }
+#pragma unroll 1
+                while (work) {
+                    const int c = __ffs(work) - 1;
+                    work &= work - 1;
+                    T se[MCH][VEC], be[MCH][VEC], xe = T(0);
+#pragma unroll
+                    for (int cc = 0; cc < CPW; ++cc) {
+                        if (cc == c) {
+                            xe = xv[cc];
+#pragma unroll
+                            for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                                for (int v = 0; v < VEC; ++v) {
+                                    se[m][v] = sv[cc][m][v];
+                                    be[m][v] = pB[cc][m][v];
+                                }
+                        }
+                    }
+                    T sn[MCH][VEC];
+                    pass_math(se, be, xe, sn);
+#pragma unroll
+                    for (int cc = 0; cc < CPW; ++cc) {
+                        if (cc == c) {
+#pragma unroll
+                            for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                                for (int v = 0; v < VEC; ++v) pj[cc][m][v].add(sn[m][v]);
+                        }
+                    }
+                    pass_out(c, se, sn);
                 }
             } else {
 #pragma unroll
