@@ -366,6 +366,15 @@ def run_batch(args):
         probs.append(pr)
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.Stream()
+    tune = None
+    if not args.no_autotune:
+        t1 = time.perf_counter()
+        d_ms, t_ms = b.autotune(probe_iters=3, psi_mode=pkg.PSI_APPR, eps=1e-50, stream=stream)
+        tune = {"seconds": time.perf_counter() - t1, "probe_iters": 3,
+                "default_probe_ms": d_ms, "tuned_probe_ms": t_ms,
+                "classes": [{k: c[k] for k in ("vec", "lanes_per_fiber", "chunks", "multirow",
+                                               "rows_per_tile", "stages", "tiles", "instances")}
+                            for c in b.classes()]}
     for _ in range(args.warmup):
         b.run(iters, pkg.PSI_APPR, 1e-50, True, stream)
     b.check(stream)
@@ -411,7 +420,8 @@ def run_batch(args):
             "config": {"workload": f"batch_{len(shapes)}_uneven", "iters": iters,
                        "x_y": "log-uniform [32,512]", "z": "{4,8,16,32,64}",
                        "total_S_elements": sum(x * y * z for x, y, z in shapes),
-                       "rows_per_tile": args.rows_per_tile or 64, "graph": True},
+                       "rows_per_tile": "autotuned per class" if tune else
+                       (args.rows_per_tile or 64), "graph": True},
             "S_updates_per_s": upd / (ms / 1e3),
             "hbm_gbs_algorithmic": alg_bytes / (ms / 1e3) / 1e9,
             "frac_of_hbm_peak": alg_bytes / (ms / 1e3) / 1e9 / peak,
@@ -419,7 +429,7 @@ def run_batch(args):
                            "S_updates_per_s": upd / (loop_ms / 1e3)},
             "speedup_vs_plain_loop": loop_ms / ms,
             "classes": b.info()["classes"], "gpu_launches": launches,
-            "setup_s": setup_s, "clocks": clk.summary()}
+            "setup_s": setup_s, "autotune": tune, "clocks": clk.summary()}
     print(json.dumps(line))
     b.close()
     return 0
@@ -638,6 +648,8 @@ def main():
                          "z in {4..64}, FP32, 150 iterations; vs a loop of the plain solver")
     ap.add_argument("--batch-n", type=int, default=512)
     ap.add_argument("--rows-per-tile", type=int, default=0)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="--batch: keep the default tile height and stage depth")
     ap.add_argument("--serve", action="store_true",
                     help="serving loop: Poisson arrivals at --rate req/s for --duration s; "
                          "p50/p99 latency, solves/s, log-marginal error vs FP64")

@@ -119,6 +119,13 @@ def build(force=False):
     return mod.build(force=force)
 
 
+class bldm_batch_class(ctypes.Structure):
+    _fields_ = [("vec", ctypes.c_int), ("lanes_per_fiber", ctypes.c_int),
+                ("chunks", ctypes.c_int), ("multirow", ctypes.c_int),
+                ("rows_per_tile", ctypes.c_int), ("stages", ctypes.c_int),
+                ("tiles", ctypes.c_size_t), ("instances", ctypes.c_size_t)]
+
+
 # Every symbol include/bldm.h declares, with (restype, argtypes).
 SIGNATURES = {
     "bldm_solve_f64": (ctypes.c_int, [_dp, _sz, _sz, _sz, ctypes.POINTER(bldm_params), _sz,
@@ -168,6 +175,10 @@ SIGNATURES = {
                                               ctypes.POINTER(_vp)]),
     "bldm_batch_info": (ctypes.c_int, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz),
                                        ctypes.POINTER(ctypes.c_uint64)]),
+    "bldm_batch_class_info": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(bldm_batch_class)]),
+    "bldm_batch_set_class": (ctypes.c_int, [_vp, ctypes.POINTER(bldm_batch_class)]),
+    "bldm_batch_autotune": (ctypes.c_int, [_vp, _sz, ctypes.c_int, ctypes.c_double, _vp, _dp,
+                                           _dp]),
     "bldm_server_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.POINTER(bldm_server_config)]),
     "bldm_server_destroy": (ctypes.c_int, [_vp]),
     "bldm_server_submit": (ctypes.c_int, [_vp, _dp, _sz, _sz, _sz, ctypes.POINTER(bldm_params),
@@ -480,6 +491,28 @@ class Batch:
         _check(lib().bldm_batch_info(self._h, ctypes.byref(nc), ctypes.byref(nb),
                                      ctypes.byref(nl)))
         return {"classes": nc.value, "device_bytes": nb.value, "launches": nl.value}
+
+    def classes(self):
+        """Launch shape of every lane-shape class (list of dicts)."""
+        out = []
+        for i in range(self.info()["classes"]):
+            c = bldm_batch_class()
+            _check(lib().bldm_batch_class_info(self._h, i, ctypes.byref(c)), "batch_class_info")
+            out.append({f: getattr(c, f) for f, _ in bldm_batch_class._fields_})
+        return out
+
+    def set_class(self, cls):
+        """Applies a class launch shape (a dict as classes() returns)."""
+        c = bldm_batch_class(**{f: int(cls.get(f, 0)) for f, _ in bldm_batch_class._fields_})
+        _check(lib().bldm_batch_set_class(self._h, ctypes.byref(c)), "batch_set_class")
+
+    def autotune(self, probe_iters=3, psi_mode=PSI_APPR, eps=1e-50, stream=None):
+        """Picks tile height and stage depth per class; returns (default_ms, tuned_ms)."""
+        d, t = ctypes.c_double(), ctypes.c_double()
+        _check(lib().bldm_batch_autotune(self._h, int(probe_iters), int(psi_mode), float(eps),
+                                         _stream_ptr(stream), ctypes.byref(d), ctypes.byref(t)),
+               "batch_autotune")
+        return d.value, t.value
 
 
 class Server:

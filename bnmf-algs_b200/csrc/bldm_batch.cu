@@ -2,7 +2,9 @@
 // different shapes solved together (bldm_batch_*).  The reference solves one
 // instance per call (bld::bld_mult_cuda, src/bld/bld_mult/bld_mult.hpp:225-324);
 // a batch runs the same iterations for all its instances in shared launches.
+#include <algorithm>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -13,6 +15,7 @@ using namespace bldm;
 struct bldm_batch {
     std::unique_ptr<Engine> eng;
     std::vector<EngineInstance> inst;
+    std::vector<EngineInstance*> ptrs;
     void* arena = nullptr;
     size_t arena_bytes = 0;
     int dtype = BLDM_F64;
@@ -38,6 +41,12 @@ int download(const void* src, size_t n, double* dst) {
     const int rc = cuda_status(cudaMemcpy(tmp.data(), src, n * 4, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) dst[i] = tmp[i];
     return rc;
+}
+
+// Re-tiles every instance from the engine's class tunings and rebuilds.
+int rebuild(bldm_batch* b, cudaStream_t st) {
+    for (auto& in : b->inst) b->eng->retile(in);
+    return b->eng->build(b->ptrs, st);
 }
 
 }  // namespace
@@ -69,16 +78,16 @@ int bldm_batch_create(bldm_batch** out, int dtype, size_t n, const size_t* xs, c
         return cuda_status(e);
     }
     b->arena_bytes = total;
-    std::vector<EngineInstance*> ptrs(n);
+    b->ptrs.resize(n);
     for (size_t i = 0; i < n; ++i) {
         b->eng->bind(b->inst[i], static_cast<char*>(b->arena) + off[i]);
-        ptrs[i] = &b->inst[i];
+        b->ptrs[i] = &b->inst[i];
     }
     for (size_t i = 0; i < n; ++i) {
         e = cudaMemset(b->inst[i].counter, 0, 16);
         if (e != cudaSuccess) return cuda_status(e);
     }
-    int rc = b->eng->build(ptrs, nullptr);
+    int rc = b->eng->build(b->ptrs, nullptr);
     if (rc) return rc;
     rc = cuda_status(cudaDeviceSynchronize());
     if (rc) return rc;
@@ -143,6 +152,155 @@ int bldm_batch_device_ptrs(bldm_batch* b, size_t idx, void** d_X, void** d_S) {
     if (d_X) *d_X = b->inst[idx].X;
     if (d_S) *d_S = b->inst[idx].S;
     return BLDM_OK;
+}
+
+int bldm_batch_class_info(const bldm_batch* b, size_t idx, bldm_batch_class* out) {
+    if (!b || !out) return BLDM_ERR_BAD_ARG;
+    ClassKey k;
+    ClassTune t;
+    size_t tiles = 0;
+    if (!b->eng->class_info(idx, &k, &t, &tiles)) return BLDM_ERR_BAD_ARG;
+    out->vec = k.vec;
+    out->lanes_per_fiber = k.lpf;
+    out->chunks = k.mch;
+    out->multirow = k.multirow ? 1 : 0;
+    out->rows_per_tile = t.rows_per_tile;
+    out->stages = t.stages;
+    out->tiles = tiles;
+    out->instances = 0;
+    for (const auto& in : b->inst)
+        if (Engine::key_of(in) == k) ++out->instances;
+    return BLDM_OK;
+}
+
+int bldm_batch_set_class(bldm_batch* b, const bldm_batch_class* c) {
+    if (!b || !c) return BLDM_ERR_BAD_ARG;
+    if ((c->rows_per_tile != 0 && c->rows_per_tile < kMinTileRows) || c->stages < 0 ||
+        c->stages == 1)
+        return BLDM_ERR_BAD_ARG;
+    ClassTune t;
+    t.rows_per_tile = c->rows_per_tile;
+    t.stages = c->stages;
+    b->eng->set_tune(ClassKey{c->vec, c->lanes_per_fiber, c->chunks, c->multirow != 0}, t);
+    return rebuild(b, nullptr);
+}
+
+int bldm_batch_autotune(bldm_batch* b, size_t probe_iters, int psi_mode, double eps,
+                        void* stream, double* default_ms, double* tuned_ms) {
+    if (!b || probe_iters == 0) return BLDM_ERR_BAD_ARG;
+    if (psi_mode < BLDM_PSI_EXACT || psi_mode > BLDM_PSI_LEGACY_CUDA) return BLDM_ERR_BAD_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t es = b->dtype == BLDM_F64 ? 8 : 4;
+    // Save S (the probes iterate it); restored before every probe and at the end.
+    size_t sbytes = 0;
+    for (const auto& in : b->inst) sbytes += in.x * in.y * in.z * es;
+    void* save = nullptr;
+    int rc = cuda_status(cudaMalloc(&save, sbytes));
+    if (rc) return rc;
+    auto copy_S = [&](bool to_save) -> int {
+        size_t off = 0;
+        for (const auto& in : b->inst) {
+            const size_t nb = in.x * in.y * in.z * es;
+            char* sv = static_cast<char*>(save) + off;
+            const cudaError_t e =
+                to_save ? cudaMemcpyAsync(sv, in.S, nb, cudaMemcpyDeviceToDevice, st)
+                        : cudaMemcpyAsync(in.S, sv, nb, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return cuda_status(e);
+            off += nb;
+        }
+        return BLDM_OK;
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    // Probe time of the current tunings; a configuration that does not fit
+    // (shared memory, ring too shallow for a multi-row stage) reports
+    // BLDM_ERR_UNSUPPORTED and is skipped.
+    auto probe = [&](double* ms) -> int {
+        int r = rebuild(b, st);
+        if (r) return r;
+        double best = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {
+            r = copy_S(false);
+            if (r) return r;
+            cudaEventRecord(e0, st);
+            r = b->eng->run(probe_iters, psi_mode, eps, false, st);
+            if (r) return r;
+            cudaEventRecord(e1, st);
+            r = b->eng->check(st);
+            if (r) return r;
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            best = std::min(best, double(t));
+        }
+        *ms = best;
+        return BLDM_OK;
+    };
+    // Classes by S elements, largest first, with their largest row count.
+    std::map<ClassKey, std::pair<size_t, size_t>> cls;  // key -> (elements, max x)
+    for (const auto& in : b->inst) {
+        auto& c = cls[Engine::key_of(in)];
+        c.first += in.x * in.y * in.z;
+        c.second = std::max(c.second, in.x);
+    }
+    std::vector<std::pair<ClassKey, std::pair<size_t, size_t>>> order(cls.begin(), cls.end());
+    std::stable_sort(order.begin(), order.end(),
+                     [](const auto& a, const auto& c) { return a.second.first > c.second.first; });
+    rc = copy_S(true);
+    double best = 0.0;
+    if (!rc) rc = probe(&best);
+    if (!rc && default_ms) *default_ms = best;
+    for (size_t ci = 0; !rc && ci < order.size(); ++ci) {
+        const ClassKey key = order[ci].first;
+        const size_t xmax = order[ci].second.second;
+        ClassTune cur = b->eng->tune_of(key);
+        for (int R : {32, 64, 128, 256, 512}) {
+            // tile heights at or above every instance's row count tile alike
+            if (R == cur.rows_per_tile || (size_t(R) >= xmax && size_t(cur.rows_per_tile) >= xmax))
+                continue;
+            b->eng->set_tune(key, ClassTune{R, cur.stages});
+            double ms = 0.0;
+            const int r = probe(&ms);
+            if (r == BLDM_ERR_UNSUPPORTED) continue;
+            if (r) {
+                rc = r;
+                break;
+            }
+            if (ms < 0.99 * best) {
+                best = ms;
+                cur.rows_per_tile = R;
+            }
+        }
+        b->eng->set_tune(key, cur);
+        for (int S : {2, 3, 4, 6, 8}) {
+            if (rc || S == cur.stages) continue;
+            b->eng->set_tune(key, ClassTune{cur.rows_per_tile, S});
+            double ms = 0.0;
+            const int r = probe(&ms);
+            if (r == BLDM_ERR_UNSUPPORTED) continue;
+            if (r) {
+                rc = r;
+                break;
+            }
+            if (ms < 0.99 * best) {
+                best = ms;
+                cur.stages = S;
+            }
+        }
+        b->eng->set_tune(key, cur);
+    }
+    if (!rc) rc = rebuild(b, st);
+    if (!rc) rc = copy_S(false);
+    if (!rc) rc = cuda_status(cudaStreamSynchronize(st));
+    if (!rc && tuned_ms) *tuned_ms = best;
+    if (rc) {
+        (void)copy_S(false);
+        cudaStreamSynchronize(st);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(save);
+    return rc;
 }
 
 int bldm_batch_info(const bldm_batch* b, size_t* n_classes, size_t* device_bytes,

@@ -66,10 +66,9 @@ int Engine::configure(EngineInstance& in, size_t x, size_t y, size_t z) const {
     c.band_w = c.wpr * c.cpw * fpw;
     c.n_bands = int((y + c.band_w - 1) / c.band_w);
     const int rps = kSweepWarps / c.wpr;
-    const int R = std::max(rps, (rows_per_tile_ + rps - 1) / rps * rps);
-    c.n_rr = int((x + R - 1) / R);
-    c.rr_base = R;
-    c.rr_extra = 0;
+    const int Rmin = std::max(rps, (kMinTileRows + rps - 1) / rps * rps);
+    in.rr_cap = int((x + Rmin - 1) / Rmin);
+    retile(in);
     const SlotLayout lay((long long)c.band_w, (long long)z, int(es_));
     in.stage_need = uint32_t(rps) * (lay.capS + lay.capX + lay.capA);
     const int KT = int(std::min<size_t>(z, kFinThreads));
@@ -81,6 +80,52 @@ int Engine::configure(EngineInstance& in, size_t x, size_t y, size_t z) const {
     return BLDM_OK;
 }
 
+ClassKey Engine::key_of(const EngineInstance& in) {
+    ClassKey k;
+    k.vec = in.cfg.vec;
+    k.lpf = in.cfg.lpf;
+    k.mch = in.cfg.mch;
+    k.multirow = in.cfg.wpr < kSweepWarps;
+    return k;
+}
+
+ClassTune Engine::tune_of(const ClassKey& k) const {
+    auto it = tune_.find(k);
+    ClassTune t = it == tune_.end() ? ClassTune{} : it->second;
+    if (t.rows_per_tile <= 0) t.rows_per_tile = rows_per_tile_;
+    return t;
+}
+
+// Row ranges of ceil(x / n_rr) rows rounded up to whole stages; since that is
+// at most the tile height, the last range is never empty.
+void Engine::retile(EngineInstance& in) const {
+    SweepCfg& c = in.cfg;
+    const int rps = kSweepWarps / c.wpr;
+    const int want = std::max(kMinTileRows, tune_of(key_of(in)).rows_per_tile);
+    const int R = std::max(rps, (want + rps - 1) / rps * rps);
+    c.n_rr = std::min(in.rr_cap, int((in.x + R - 1) / R));
+    c.rr_base = int((in.x + c.n_rr - 1) / c.n_rr);
+    c.rr_base = (c.rr_base + rps - 1) / rps * rps;
+    c.rr_extra = 0;
+}
+
+bool Engine::class_info(size_t i, ClassKey* k, ClassTune* t, size_t* tiles) const {
+    if (i >= classes_.size()) return false;
+    const ShapeClass& c = classes_[i];
+    ClassKey key;
+    key.vec = c.vec;
+    key.lpf = c.lpf;
+    key.mch = c.mch;
+    key.multirow = c.multirow;
+    if (k) *k = key;
+    if (t) {
+        *t = tune_of(key);
+        t->stages = c.stages;
+    }
+    if (tiles) *tiles = c.tiles.size();
+    return true;
+}
+
 InstanceBytes Engine::bytes(const EngineInstance& in) const {
     const SweepCfg& c = in.cfg;
     InstanceBytes b;
@@ -88,14 +133,14 @@ InstanceBytes Engine::bytes(const EngineInstance& in) const {
     b.S = in.x * in.y * in.z * es_;
     b.alpha = in.x * 8;
     b.beta = in.z * 8;
-    b.pjk = size_t(c.n_rr) * in.y * in.z * 8;
+    b.pjk = size_t(in.rr_cap) * in.y * in.z * 8;
     b.ipk = size_t(c.n_bands) * in.x * in.z * 8;
     b.psiB = in.y * in.z * es_;
     b.psiA = in.x * in.z * es_;
     b.psiAS = in.z * es_;
     b.asum = size_t(c.n_ablk) * in.z * 8;
     b.counter = 16;
-    b.delta = size_t(c.n_rr) * c.n_bands * 16;
+    b.delta = size_t(in.rr_cap) * c.n_bands * 16;
     b.rel = 8;
     return b;
 }
@@ -237,6 +282,8 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
         if (s < 2) s = long((220 * 1024 - std::min<size_t>(fixed, 220 * 1024)) / per_stage);
         if (s < 2) return BLDM_ERR_UNSUPPORTED;
         k.stages = int(std::min(8L, s));
+        const ClassTune t = tune_of(ClassKey{k.vec, k.lpf, k.mch, k.multirow});
+        if (t.stages >= 2) k.stages = std::min(k.stages, t.stages);
         k.smem = size_t(k.stages) * per_stage + fixed;
         for (int upd = 0; upd < 2; ++upd)
             for (int ap = 0; ap < 2; ++ap) {
@@ -258,6 +305,22 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
             return BLDM_ERR_UNSUPPORTED;
         for (int rr = 0; rr < c.n_rr; ++rr)
             for (int b = 0; b < c.n_bands; ++b) k.tiles.push_back(BatchTile{int(n), b, rr, 0});
+    }
+    // Largest tiles first: blocks start in index order as slots free up, so a
+    // class grid of several waves ends with its smallest tiles (longest
+    // processing time first).  The order depends only on the shapes.
+    for (auto& k : classes_) {
+        auto work = [&](const BatchTile& t) {
+            const EngineInstance& in = *insts[size_t(t.inst)];
+            const SweepCfg& c = in.cfg;
+            const long long r0 = (long long)t.rr * c.rr_base;
+            const long long rows = std::min<long long>(c.rr_base, (long long)in.x - r0);
+            const long long cols =
+                std::min<long long>(c.band_w, (long long)in.y - (long long)t.band * c.band_w);
+            return rows * cols * (long long)in.z;
+        };
+        std::stable_sort(k.tiles.begin(), k.tiles.end(),
+                         [&](const BatchTile& a, const BatchTile& b) { return work(a) > work(b); });
     }
     // Device tables: SweepInst[n] | FinInst[n] | block_off[n+1] | err | tiles per class.
     const size_t n = insts.size();

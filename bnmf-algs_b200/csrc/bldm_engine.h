@@ -21,10 +21,30 @@
 
 namespace bldm {
 
+// Lane-shape class of an instance: the sweep kernel it runs on.
+struct ClassKey {
+    int vec = 0, lpf = 0, mch = 0;
+    bool multirow = false;  // fewer than 8 warps per row (narrow rows share a stage)
+    bool operator<(const ClassKey& o) const {
+        return std::tie(vec, lpf, mch, multirow) < std::tie(o.vec, o.lpf, o.mch, o.multirow);
+    }
+    bool operator==(const ClassKey& o) const {
+        return vec == o.vec && lpf == o.lpf && mch == o.mch && multirow == o.multirow;
+    }
+};
+
+// Tunable launch shape of a class: rows of S per tile (the tile height) and
+// the depth of the bulk-copy stage ring (0 = as deep as shared memory allows).
+struct ClassTune {
+    int rows_per_tile = 0;
+    int stages = 0;
+};
+
 // One instance: shape, derived geometry and device buffers.
 struct EngineInstance {
     size_t x = 0, y = 0, z = 0;
     SweepCfg cfg{};      // lane shape, wpr, band_w, n_bands, n_rr, rr_base, n_ablk...
+    int rr_cap = 0;      // row ranges the partial buffers hold (any tile height >= kMinTileRows)
     int nbB = 0;         // finalize blocks for psi(beta_eph)
     uint32_t stage_need = 0;
     // device buffers (owned by the engine's user)
@@ -49,6 +69,9 @@ struct InstanceBytes {
     size_t total(size_t align) const;
 };
 
+// Smallest tile height a tuning may set; partial buffers are sized for it.
+constexpr int kMinTileRows = 32;
+
 class Engine {
   public:
     Engine(int dtype, int rows_per_tile);
@@ -58,6 +81,17 @@ class Engine {
 
     // Geometry of an instance of this shape (no device work).
     int configure(EngineInstance& in, size_t x, size_t y, size_t z) const;
+    // Re-derives the row ranges of a configured instance from its class's
+    // current tile height (within the capacity its buffers were sized for).
+    void retile(EngineInstance& in) const;
+    static ClassKey key_of(const EngineInstance& in);
+    // Per-class launch shape; takes effect for instances configured or
+    // retiled afterwards and at the next build.
+    void set_tune(const ClassKey& k, const ClassTune& t) { tune_[k] = t; }
+    ClassTune tune_of(const ClassKey& k) const;
+    int default_rows_per_tile() const { return rows_per_tile_; }
+    // Launch shape in effect for class i of the last build.
+    bool class_info(size_t i, ClassKey* k, ClassTune* t, size_t* tiles) const;
     InstanceBytes bytes(const EngineInstance& in) const;
     // Points the instance's buffers into `base` (InstanceBytes layout, 256-aligned).
     void bind(EngineInstance& in, void* base) const;
@@ -114,6 +148,7 @@ class Engine {
     cudaEvent_t fork_ = nullptr;
     uint64_t launches_ = 0;
     std::map<std::tuple<size_t, int, uint64_t>, cudaGraphExec_t> graphs_;
+    std::map<ClassKey, ClassTune> tune_;
 };
 
 }  // namespace bldm

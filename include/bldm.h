@@ -241,13 +241,17 @@ int bldm_log_marginal_S(const void* d_S, int dtype, size_t x, size_t y, size_t z
 /* ------------------------------------------------------------------------
  * Batched solver: many independent instances of different shapes (x, y, z
  * each) solved together.  No counterpart in the reference, which solves one
- * instance per call; each instance's result is the one bldm_plan_run gives
- * for it alone (same tiling, same reduction order).  One iteration of every
- * instance is one fused-sweep launch per lane-shape class (instances whose z
- * maps to the same kernel), the classes concurrent on forked streams, and one
- * finalize launch for all instances; with use_graph the whole run is captured
- * once per (iters, psi_mode, eps) into a CUDA graph and replayed.
- * rows_per_tile (0 = 64) sets the rows of one CTA tile (the autotuner's knob).
+ * instance per call.  An instance's tiling depends only on its own shape and
+ * its class's launch shape, so its result does not depend on the other
+ * instances of the batch; it agrees with bldm_plan_run's to rounding (the
+ * partial sums are grouped by tile).  One iteration of every instance is one
+ * fused-sweep launch per lane-shape class (instances whose z maps to the same
+ * kernel), the classes concurrent on forked streams, and one finalize launch
+ * for all instances; with use_graph the whole run is captured once per
+ * (iters, psi_mode, eps) into a CUDA graph and replayed.
+ * rows_per_tile (0 = 64) is the default tile height (rows of S per CTA tile)
+ * of every class; bldm_batch_autotune picks it and the stage-ring depth per
+ * class from timed probe runs on the batch's own data.
  * X, S0 and S_out are host FP64 arrays (converted for BLDM_F32 storage).
  * ---------------------------------------------------------------------- */
 typedef struct bldm_batch bldm_batch;
@@ -269,6 +273,33 @@ int bldm_batch_get(bldm_batch* batch, size_t idx, double* S_out, double* rel_cha
 int bldm_batch_device_ptrs(bldm_batch* batch, size_t idx, void** d_X, void** d_S);
 int bldm_batch_info(const bldm_batch* batch, size_t* n_classes, size_t* device_bytes,
                     uint64_t* launches);
+
+/* Launch shape of one lane-shape class of a batch. */
+typedef struct bldm_batch_class {
+    int vec;              /* elements per lane access */
+    int lanes_per_fiber;  /* lanes sharing one (i,j) fiber */
+    int chunks;           /* vec-element chunks per lane and fiber */
+    int multirow;         /* 1: narrow rows, several rows per stage */
+    int rows_per_tile;    /* tile height: rows of S per CTA tile */
+    int stages;           /* bulk-copy ring depth (row segments of S in flight per CTA) */
+    size_t tiles;         /* CTA tiles per sweep launch */
+    size_t instances;     /* instances of the batch in this class */
+} bldm_batch_class;
+/* Class idx (< n_classes of bldm_batch_info) as the last build laid it out. */
+int bldm_batch_class_info(const bldm_batch* batch, size_t idx, bldm_batch_class* out);
+/* Sets the launch shape of the class with c's (vec, lanes_per_fiber, chunks,
+ * multirow); rows_per_tile >= 32 (0 = the batch default), stages >= 2 or 0
+ * (= as deep as shared memory allows).  Re-tiles and rebuilds the batch. */
+int bldm_batch_set_class(bldm_batch* batch, const bldm_batch_class* c);
+/* Autotuner: for each class, largest first, tries tile heights
+ * {32, 64, 128, 256, 512} and stage depths {2, 3, 4, 6, 8}, timing
+ * probe_iters iterations of the whole batch (CUDA events, best of two) from
+ * the current S, and keeps a change when the batch gets at least 1% faster.
+ * S is saved on the device and restored afterwards, so the call does not
+ * change the solution.  Call after bldm_batch_set of every instance.
+ * default_ms / tuned_ms (nullable): probe time before and after. */
+int bldm_batch_autotune(bldm_batch* batch, size_t probe_iters, int psi_mode, double eps,
+                        void* stream, double* default_ms, double* tuned_ms);
 
 /* ------------------------------------------------------------------------
  * Serving loop with continuous batching.  No counterpart in the reference.

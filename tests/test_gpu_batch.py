@@ -144,3 +144,56 @@ def test_batch_rejects_bad_input(bldm):
     with pytest.raises(ValueError):
         b.set(3, np.ones((4, 5)), np.ones(4), np.ones(3))
     b.close()
+
+
+def test_autotune_keeps_solution_and_reports_classes(bldm, oracle, workloads):
+    """The autotuner times probe runs but restores S: the tuned batch then
+    solves to the same tolerance, and every class reports a legal shape."""
+    probs = _problems(workloads, oracle, SHAPES, 60)
+    b = bldm.Batch(SHAPES, dtype=bldm.F64)
+    for k, (X, a, be, S0) in enumerate(probs):
+        b.set(k, X, a, be, S0)
+    before = [b.get(k)[0] for k in range(len(SHAPES))]
+    d_ms, t_ms = b.autotune(probe_iters=2)
+    assert d_ms > 0 and 0 < t_ms <= d_ms
+    for k in range(len(SHAPES)):
+        np.testing.assert_array_equal(b.get(k)[0], before[k])
+    cls = b.classes()
+    assert sum(c["instances"] for c in cls) == len(SHAPES)
+    for c in cls:
+        assert c["rows_per_tile"] >= 32 and c["stages"] >= 2 and c["tiles"] >= 1
+    b.run(10, use_graph=False)
+    b.check()
+    for k, (X, a, be, S0) in enumerate(probs):
+        ref = oracle.bld_mult(X, SHAPES[k][2], a, be, 10, oracle.PSI_APPR, 1e-50, S0=S0)
+        assert rel_err(b.get(k)[0], ref) <= 1e-9, SHAPES[k]
+    b.close()
+
+
+def test_class_shape_applies_alone_and_in_mix(bldm, oracle, workloads):
+    """With the same class launch shapes an instance gives bitwise the same
+    result alone and in a mix; a tile height below 32 is rejected."""
+    probs = _problems(workloads, oracle, SHAPES, 80)
+    mix = bldm.Batch(SHAPES, dtype=bldm.F32)
+    for k, (X, a, be, S0) in enumerate(probs):
+        mix.set(k, X, a, be, S0)
+    shapes = []
+    for c in mix.classes():
+        c = dict(c, rows_per_tile=32, stages=2)
+        mix.set_class(c)
+        shapes.append(c)
+    with pytest.raises(ValueError):
+        mix.set_class(dict(shapes[0], rows_per_tile=16))
+    mix.run(8, use_graph=True, stream=None)
+    mix.check()
+    for k in (3, 7):
+        alone = bldm.Batch([SHAPES[k]], dtype=bldm.F32)
+        X, a, be, S0 = probs[k]
+        alone.set(0, X, a, be, S0)
+        for c in shapes:
+            alone.set_class(c)
+        alone.run(8, use_graph=False)
+        alone.check()
+        np.testing.assert_array_equal(alone.get(0)[0], mix.get(k)[0])
+        alone.close()
+    mix.close()
