@@ -89,7 +89,9 @@ class bldm_server_stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("submitted", "completed", "failed", "rounds",
                                               "iterations")] + \
                [(n, ctypes.c_size_t) for n in ("active", "queued", "bytes_in_use", "bytes_peak",
-                                              "budget")]
+                                              "budget")] + \
+               [("gpu_ms", ctypes.c_double), ("host_ms", ctypes.c_double),
+                ("retiring", ctypes.c_size_t)]
 
 
 _lib = None
@@ -560,12 +562,13 @@ class Server:
     def wait(self, rid, timeout=120.0):
         return lib().bldm_server_wait(self._h, rid, float(timeout)) == OK
 
-    def fetch(self, rid):
-        """(S or None, stats dict); S is None when the request failed."""
+    def fetch(self, rid, want_S=True):
+        """(S or None, stats dict); S is None when the request failed or want_S is False."""
         x, y, z = self._shapes.pop(rid)
-        S = np.empty((x, y, z))
+        S = np.empty((x, y, z)) if want_S else None
         rs = bldm_request_stats()
-        rc = lib().bldm_server_fetch(self._h, rid, S.ctypes.data_as(_dp), ctypes.byref(rs))
+        rc = lib().bldm_server_fetch(self._h, rid, S.ctypes.data_as(_dp) if want_S else None,
+                                     ctypes.byref(rs))
         stats = {"queue_ms": rs.queue_ms, "latency_ms": rs.latency_ms,
                  "iterations": rs.iterations, "rel_change": rs.rel_change,
                  "log_marginal": rs.log_marginal, "status": rs.status}

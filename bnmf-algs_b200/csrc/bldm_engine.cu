@@ -449,13 +449,25 @@ int Engine::launch_finalize(int plus_appr, int minus_appr, cudaStream_t st) {
     return cuda_status(cudaGetLastError());
 }
 
-int Engine::launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st) {
+int Engine::prime(int psi_mode, cudaStream_t st) {
+    if (psi_mode < BLDM_PSI_EXACT || psi_mode > BLDM_PSI_LEGACY_CUDA) return BLDM_ERR_BAD_ARG;
+    if (insts_.empty()) return BLDM_OK;
+    const int rc = launch_sweeps(false, true, false, 0.0, st);
+    if (rc) return rc;
+    return launch_finalize(psi_mode != BLDM_PSI_EXACT, psi_mode == BLDM_PSI_APPR, st);
+}
+
+int Engine::launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st,
+                            bool prime) {
     const int plus_appr = psi_mode != BLDM_PSI_EXACT;
     const int minus_appr = psi_mode == BLDM_PSI_APPR;
-    int rc = launch_sweeps(false, true, false, eps, st);
-    if (rc) return rc;
-    rc = launch_finalize(plus_appr, minus_appr, st);
-    if (rc) return rc;
+    int rc = BLDM_OK;
+    if (prime) {
+        rc = launch_sweeps(false, true, false, eps, st);
+        if (rc) return rc;
+        rc = launch_finalize(plus_appr, minus_appr, st);
+        if (rc) return rc;
+    }
     for (size_t it = 0; it < iters; ++it) {
         rc = launch_sweeps(true, plus_appr != 0, it + 1 == iters, eps, st);
         if (rc) return rc;
@@ -465,18 +477,19 @@ int Engine::launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t
     return BLDM_OK;
 }
 
-int Engine::run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStream_t st) {
+int Engine::run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStream_t st,
+                bool prime) {
     if (psi_mode < BLDM_PSI_EXACT || psi_mode > BLDM_PSI_LEGACY_CUDA) return BLDM_ERR_BAD_ARG;
     if (iters == 0 || insts_.empty()) return BLDM_OK;
-    if (!use_graph || st == nullptr) return launch_sequence(iters, psi_mode, eps, st);
+    if (!use_graph || st == nullptr) return launch_sequence(iters, psi_mode, eps, st, prime);
     uint64_t eb;
     std::memcpy(&eb, &eps, sizeof eb);
-    const auto key = std::make_tuple(iters, psi_mode, eb);
+    const auto key = std::make_tuple(iters, psi_mode, eb, prime);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
         const uint64_t l0 = launches_;
         ENG_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        const int rc = launch_sequence(iters, psi_mode, eps, st);
+        const int rc = launch_sequence(iters, psi_mode, eps, st, prime);
         cudaGraph_t g = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(st, &g);
         launches_ = l0;
@@ -492,7 +505,7 @@ int Engine::run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStre
         it = graphs_.emplace(key, exec).first;
     }
     ENG_CU(cudaGraphLaunch(it->second, st));
-    launches_ += (iters + 1) * (classes_.size() + 1);
+    launches_ += (iters + (prime ? 1 : 0)) * (classes_.size() + 1);
     return BLDM_OK;
 }
 

@@ -100,8 +100,13 @@ class Engine {
     // stay valid until the next build.  Clears the per-instance counters on st.
     int build(const std::vector<EngineInstance*>& insts, cudaStream_t st);
     // Runs `iters` iterations of every instance (from the S currently in the
-    // buffers), tracking the relative change of the last one.
-    int run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStream_t st);
+    // buffers), tracking the relative change of the last one.  With prime,
+    // the run first computes the axis sums and digamma tables of the current
+    // S; without, it relies on those the last update (or prime()) left.
+    int run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStream_t st,
+            bool prime = true);
+    // Axis sums and digamma tables of the current S of every instance.
+    int prime(int psi_mode, cudaStream_t st);
     int check(cudaStream_t st);
 
     int dtype() const { return dtype_; }
@@ -123,7 +128,7 @@ class Engine {
         cudaStream_t stream = nullptr;
         cudaEvent_t done = nullptr;
     };
-    int launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st);
+    int launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st, bool prime);
     int launch_sweeps(bool update, bool appr, bool track, double eps, cudaStream_t st);
     int launch_finalize(int plus_appr, int minus_appr, cudaStream_t st);
     void free_tables();
@@ -147,7 +152,7 @@ class Engine {
     int fin_blocks_ = 0;
     cudaEvent_t fork_ = nullptr;
     uint64_t launches_ = 0;
-    std::map<std::tuple<size_t, int, uint64_t>, cudaGraphExec_t> graphs_;
+    std::map<std::tuple<size_t, int, uint64_t, bool>, cudaGraphExec_t> graphs_;
     std::map<ClassKey, ClassTune> tune_;
 };
 

@@ -310,9 +310,13 @@ int bldm_batch_autotune(bldm_batch* batch, size_t probe_iters, int psi_mode, dou
  * requests per round in shared launches, and retires a request when the
  * relative change of S (sum|S_n - S_{n-1}| / sum|S_n| over its last
  * iteration) falls below tol or it has run max_iter iterations (rounded up to
- * a whole round).  Retirement copies S to the host and computes
- * log_marginal_S on the device (FP64).  A request's result does not depend
- * on the other requests being served.
+ * a whole round).  Newly admitted requests get their axis sums on their own
+ * before joining the round; the others carry theirs over from the previous
+ * round.  Retirement runs on a second thread and stream, so the rounds go on
+ * meanwhile: it copies S to the host (in the storage type; fetch converts to
+ * FP64), computes log_marginal_S on the device (FP64) and frees the request's
+ * device memory.  A request's result does not depend on the other requests
+ * being served.
  * ---------------------------------------------------------------------- */
 typedef struct bldm_server bldm_server;
 typedef struct bldm_server_config {
@@ -337,6 +341,9 @@ typedef struct bldm_request_stats {
 typedef struct bldm_server_stats {
     uint64_t submitted, completed, failed, rounds, iterations;
     size_t active, queued, bytes_in_use, bytes_peak, budget;
+    double gpu_ms;           /* device time of the rounds (CUDA events) */
+    double host_ms;          /* worker time between rounds (admission, tables) */
+    size_t retiring;         /* requests finished on the device, results in flight */
 } bldm_server_stats;
 int bldm_server_create(bldm_server** server, const bldm_server_config* config);
 /* Stops the worker; requests still active or queued are dropped. */
