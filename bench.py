@@ -260,6 +260,33 @@ def run_ours(args):
                 "iteration_ms": iter_ms,
                 "iteration_frac": alg_bytes / (iter_ms / 1e3) / 1e9 / peak}
 
+    # The same solve with skip_zero_rows: bitwise the same S; after the first
+    # update, rows whose band segment of X is all zero are neither read nor
+    # written and zeros are not stored again.  Its rate counts all x*y*z
+    # updates of an iteration; the roofline above stays the streaming kernel's.
+    plan_skip = pkg.Plan(x, y, z, dtype, skip_zero_rows=True)
+    dS2 = torch.empty_like(dS)
+    plan_skip.init_S(dX, dS2, seed=0)
+    for _ in range(2):
+        plan_skip.run(dX, dalpha, dbeta, dS2, iters, mode, 1e-50, stream)
+    plan_skip.check(stream)
+    n_skip = max(1, args.steps // 3)
+    e0.record(stream)
+    for _ in range(n_skip):
+        plan_skip.run(dX, dalpha, dbeta, dS2, iters, mode, 1e-50, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plan_skip.check(stream)
+    skip_ms = e0.elapsed_time(e1) / n_skip
+    skip_kern, _ = plan_skip.profile(dX, dalpha, dbeta, dS2, 20, mode, 1e-50, stream)
+    zero_row_skip = {"value": upd_step / (skip_ms / 1e3), "unit": "S-updates/s",
+                     "ms_per_step": skip_ms, "speedup": ms_max / skip_ms,
+                     "update_kernel_ms": skip_kern, "steps": n_skip,
+                     "fibers_with_X_nonzero": float(np.mean(X != 0)),
+                     "note": "bldm_tuning.skip_zero_rows; bitwise the same S"}
+    plan_skip.close()
+    del dS2
+
     # End to end through the public host-buffer C ABI (pinned host buffers,
     # H2D of X and S0 and D2H of S inside every step).
     hX = torch.as_tensor(X.astype(np.float64 if f64 else np.float32)).pin_memory()
@@ -308,7 +335,7 @@ def run_ours(args):
                            "l2": "inputs larger than L2 (S is 512 MiB in f64)",
                            "parallelism": "replicas" if world > 1 else "single GPU"},
                 "hbm_gbs_iteration": alg_bytes / (ms_max / 1e3 / iters) / 1e9,
-                "roofline": roofline, "cpu_baseline": cpu,
+                "roofline": roofline, "zero_row_skip": zero_row_skip, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "S-updates/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
                 "gpu_launches": launches, "clocks": clk.summary()}

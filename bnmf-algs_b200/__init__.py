@@ -63,7 +63,7 @@ class bldm_params(ctypes.Structure):
 
 class bldm_tuning(ctypes.Structure):
     _fields_ = [("stages", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
-                ("row_ranges", ctypes.c_int)]
+                ("row_ranges", ctypes.c_int), ("skip_zero_rows", ctypes.c_int)]
 
 
 class bldm_stats(ctypes.Structure):
@@ -298,12 +298,14 @@ def _stream_ptr(stream):
 class Plan:
     """bldm_plan: workspace for one (x, y, z, dtype); runs on device tensors."""
 
-    def __init__(self, x, y, z, dtype=F64, stages=0, ctas_per_sm=0, row_ranges=0):
+    def __init__(self, x, y, z, dtype=F64, stages=0, ctas_per_sm=0, row_ranges=0,
+                 skip_zero_rows=False):
         self._h = ctypes.c_void_p()
         self.shape = (x, y, z)
         self.dtype = dtype
-        if stages or ctas_per_sm or row_ranges:
-            t = bldm_tuning(int(stages), int(ctas_per_sm), int(row_ranges))
+        if stages or ctas_per_sm or row_ranges or skip_zero_rows:
+            t = bldm_tuning(int(stages), int(ctas_per_sm), int(row_ranges),
+                            1 if skip_zero_rows else 0)
             _check(lib().bldm_plan_create_tuned(ctypes.byref(self._h), x, y, z, dtype,
                                                 ctypes.byref(t)), "plan_create_tuned")
         else:
@@ -312,7 +314,8 @@ class Plan:
     def tuning(self):
         t = bldm_tuning()
         _check(lib().bldm_plan_get_tuning(self._h, ctypes.byref(t)))
-        return {"stages": t.stages, "ctas_per_sm": t.ctas_per_sm, "row_ranges": t.row_ranges}
+        return {"stages": t.stages, "ctas_per_sm": t.ctas_per_sm, "row_ranges": t.row_ranges,
+                "skip_zero_rows": bool(t.skip_zero_rows)}
 
     def close(self):
         if self._h:

@@ -19,6 +19,7 @@ struct bldm_batch {
     void* arena = nullptr;
     size_t arena_bytes = 0;
     int dtype = BLDM_F64;
+    bool clean = false;  // every instance has been updated since its S was set
     ~bldm_batch() {
         eng.reset();
         if (arena) cudaFree(arena);
@@ -85,6 +86,9 @@ int bldm_batch_create(bldm_batch** out, int dtype, size_t n, const size_t* xs, c
     }
     for (size_t i = 0; i < n; ++i) {
         e = cudaMemset(b->inst[i].counter, 0, 16);
+        // empty row lists until bldm_batch_set fills them from X
+        if (e == cudaSuccess)
+            e = cudaMemset(b->inst[i].nz_cnt, 0, b->eng->bytes(b->inst[i]).nzc);
         if (e != cudaSuccess) return cuda_status(e);
     }
     int rc = b->eng->build(b->ptrs, nullptr);
@@ -108,14 +112,21 @@ int bldm_batch_set(bldm_batch* b, size_t idx, const double* X, const double* alp
     for (size_t e = 0; e < in.x * in.y; ++e)
         if (!(X[e] >= 0.0)) return BLDM_ERR_NEG_X;
     const bool f64 = b->dtype == BLDM_F64;
+    b->clean = false;
     int rc = f64 ? upload<double>(X, in.x * in.y, in.X) : upload<float>(X, in.x * in.y, in.X);
+    if (rc) return rc;
+    rc = b->eng->set_row_lists(in, nullptr);
     if (rc) return rc;
     rc = cuda_status(cudaMemcpy(in.alpha, alpha, in.x * 8, cudaMemcpyHostToDevice));
     if (rc) return rc;
     rc = cuda_status(cudaMemcpy(in.beta, beta, in.z * 8, cudaMemcpyHostToDevice));
     if (rc) return rc;
     const size_t ns = in.x * in.y * in.z;
-    if (S0) return f64 ? upload<double>(S0, ns, in.S) : upload<float>(S0, ns, in.S);
+    if (S0) {
+        rc = f64 ? upload<double>(S0, ns, in.S) : upload<float>(S0, ns, in.S);
+        if (rc) return rc;
+        return cuda_status(cudaDeviceSynchronize());
+    }
     rc = launch_init_S(b->dtype, in.X, in.S, (long long)(in.x * in.y), (long long)in.z, seed,
                        nullptr);
     if (rc) return rc;
@@ -125,7 +136,10 @@ int bldm_batch_set(bldm_batch* b, size_t idx, const double* X, const double* alp
 int bldm_batch_run(bldm_batch* b, size_t iters, int psi_mode, double eps, int use_graph,
                    void* stream) {
     if (!b) return BLDM_ERR_BAD_ARG;
-    return b->eng->run(iters, psi_mode, eps, use_graph != 0, static_cast<cudaStream_t>(stream));
+    const int rc = b->eng->run(iters, psi_mode, eps, use_graph != 0,
+                               static_cast<cudaStream_t>(stream), true, b->clean);
+    if (rc == BLDM_OK && iters > 0) b->clean = true;
+    return rc;
 }
 
 int bldm_batch_check(bldm_batch* b, void* stream) {
@@ -292,6 +306,7 @@ int bldm_batch_autotune(bldm_batch* b, size_t probe_iters, int psi_mode, double 
     if (!rc) rc = rebuild(b, st);
     if (!rc) rc = copy_S(false);
     if (!rc) rc = cuda_status(cudaStreamSynchronize(st));
+    b->clean = false;  // S is the one from before the probes
     if (!rc && tuned_ms) *tuned_ms = best;
     if (rc) {
         (void)copy_S(false);

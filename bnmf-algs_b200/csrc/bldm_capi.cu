@@ -259,6 +259,7 @@ int bldm_plan_get_tuning(const bldm_plan* plan, bldm_tuning* out) {
     out->stages = plan->impl.cfg.stages;
     out->ctas_per_sm = plan->impl.cfg.ctas_per_sm;
     out->row_ranges = plan->impl.cfg.n_rr;
+    out->skip_zero_rows = plan->impl.skip_zero ? 1 : 0;
     return BLDM_OK;
 }
 

@@ -28,15 +28,15 @@ int sms_of_current_device() {
 
 size_t InstanceBytes::total(size_t align) const {
     const size_t parts[] = {X, S, alpha, beta, pjk, ipk, psiB, psiA, psiAS, asum, counter, delta,
-                            rel};
+                            rel, nzr, nzc};
     size_t t = 0;
     for (size_t p : parts) t += (p + align - 1) / align * align;
     return t;
 }
 
-Engine::Engine(int dtype, int rows_per_tile)
+Engine::Engine(int dtype, int rows_per_tile, bool skip_zero)
     : dtype_(dtype), es_(dtype == BLDM_F64 ? 8 : 4),
-      rows_per_tile_(rows_per_tile > 0 ? rows_per_tile : 64),
+      rows_per_tile_(rows_per_tile > 0 ? rows_per_tile : 64), skip_zero_(skip_zero),
       num_sms_(sms_of_current_device()) {
     cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming);
 }
@@ -142,7 +142,14 @@ InstanceBytes Engine::bytes(const EngineInstance& in) const {
     b.counter = 16;
     b.delta = size_t(in.rr_cap) * c.n_bands * 16;
     b.rel = 8;
+    b.nzr = size_t(c.n_bands) * in.x * 4;
+    b.nzc = size_t(c.n_bands) * (in.x + 1) * 4;
     return b;
+}
+
+int Engine::set_row_lists(EngineInstance& in, cudaStream_t st) const {
+    return launch_nz_rows(dtype_, in.X, (long long)in.x, (long long)in.y, in.cfg.band_w,
+                          in.cfg.n_bands, in.nz_rows, in.nz_cnt, st);
 }
 
 void Engine::bind(EngineInstance& in, void* base) const {
@@ -166,6 +173,8 @@ void Engine::bind(EngineInstance& in, void* base) const {
     in.counter = reinterpret_cast<unsigned*>(take(b.counter));
     in.delta = reinterpret_cast<double*>(take(b.delta));
     in.rel = reinterpret_cast<double*>(take(b.rel));
+    in.nz_rows = reinterpret_cast<int*>(take(b.nzr));
+    in.nz_cnt = reinterpret_cast<int*>(take(b.nzc));
 }
 
 void Engine::free_tables() {
@@ -184,7 +193,7 @@ void Engine::drop_graphs() {
 
 template <typename T>
 static void fill_tables(const std::vector<EngineInstance*>& insts, std::vector<char>& host,
-                        size_t o_sinst, size_t o_finst) {
+                        size_t o_sinst, size_t o_finst, bool skip_zero) {
     SweepInst<T>* si = reinterpret_cast<SweepInst<T>*>(host.data() + o_sinst);
     FinInst<T>* fi = reinterpret_cast<FinInst<T>*>(host.data() + o_finst);
     for (size_t n = 0; n < insts.size(); ++n) {
@@ -199,6 +208,8 @@ static void fill_tables(const std::vector<EngineInstance*>& insts, std::vector<c
         s.part_pjk = in.part_pjk;
         s.part_ipk = in.part_ipk;
         s.delta_part = in.delta;
+        s.nz_rows = skip_zero ? in.nz_rows : nullptr;
+        s.nz_cnt = skip_zero ? in.nz_cnt : nullptr;
         s.x = (long long)in.x;
         s.y = (long long)in.y;
         s.z = (long long)in.z;
@@ -285,10 +296,10 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
         const ClassTune t = tune_of(ClassKey{k.vec, k.lpf, k.mch, k.multirow});
         if (t.stages >= 2) k.stages = std::min(k.stages, t.stages);
         k.smem = size_t(k.stages) * per_stage + fixed;
-        for (int upd = 0; upd < 2; ++upd)
+        for (int mode = SWEEP_SUMS; mode <= SWEEP_COMPACT; ++mode)
             for (int ap = 0; ap < 2; ++ap) {
-                void* fn =
-                    pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, upd != 0, ap != 0, true, k.multirow);
+                void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, mode, ap != 0, true,
+                                         k.multirow);
                 if (!fn) return BLDM_ERR_UNSUPPORTED;
                 const int rc_attr = ensure_smem_attr(fn, k.smem);
                 if (rc_attr) return rc_attr;
@@ -360,9 +371,9 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
     std::vector<char> hv;  // fill_tables works on a vector view of the staging buffer
     hv.resize(o_boff);
     if (dtype_ == BLDM_F64)
-        fill_tables<double>(insts, hv, o_sinst, o_finst);
+        fill_tables<double>(insts, hv, o_sinst, o_finst, skip_zero_);
     else
-        fill_tables<float>(insts, hv, o_sinst, o_finst);
+        fill_tables<float>(insts, hv, o_sinst, o_finst, skip_zero_);
     std::memcpy(host, hv.data(), o_boff);
     int* boff = reinterpret_cast<int*>(host + o_boff);
     fin_blocks_ = 0;
@@ -401,14 +412,16 @@ static void launch_class_kernel(void* fn, unsigned grid, size_t smem, cudaStream
     reinterpret_cast<void (*)(const BatchSweepParams<T>)>(fn)<<<grid, kSweepThreads, smem, s>>>(p);
 }
 
-int Engine::launch_sweeps(bool update, bool appr, bool track, double eps, cudaStream_t st) {
+int Engine::launch_sweeps(bool update, bool appr, bool track, double eps, cudaStream_t st,
+                          bool clean) {
     const bool fork = classes_.size() > 1;
     if (fork) ENG_CU(cudaEventRecord(fork_, st));
     for (auto& k : classes_) {
         if (k.tiles.empty()) continue;
         cudaStream_t s = fork ? k.stream : st;
         if (fork) ENG_CU(cudaStreamWaitEvent(s, fork_, 0));
-        void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, update, appr, true, k.multirow);
+        const int mode = !update ? SWEEP_SUMS : (clean ? SWEEP_COMPACT : SWEEP_UPDATE);
+        void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, mode, appr, true, k.multirow);
         if (dtype_ == BLDM_F64)
             launch_class_kernel<double>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_,
                                         k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track);
@@ -452,24 +465,25 @@ int Engine::launch_finalize(int plus_appr, int minus_appr, cudaStream_t st) {
 int Engine::prime(int psi_mode, cudaStream_t st) {
     if (psi_mode < BLDM_PSI_EXACT || psi_mode > BLDM_PSI_LEGACY_CUDA) return BLDM_ERR_BAD_ARG;
     if (insts_.empty()) return BLDM_OK;
-    const int rc = launch_sweeps(false, true, false, 0.0, st);
+    const int rc = launch_sweeps(false, true, false, 0.0, st, false);
     if (rc) return rc;
     return launch_finalize(psi_mode != BLDM_PSI_EXACT, psi_mode == BLDM_PSI_APPR, st);
 }
 
 int Engine::launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st,
-                            bool prime) {
+                            bool prime, bool clean_first) {
     const int plus_appr = psi_mode != BLDM_PSI_EXACT;
     const int minus_appr = psi_mode == BLDM_PSI_APPR;
     int rc = BLDM_OK;
     if (prime) {
-        rc = launch_sweeps(false, true, false, eps, st);
+        rc = launch_sweeps(false, true, false, eps, st, false);
         if (rc) return rc;
         rc = launch_finalize(plus_appr, minus_appr, st);
         if (rc) return rc;
     }
     for (size_t it = 0; it < iters; ++it) {
-        rc = launch_sweeps(true, plus_appr != 0, it + 1 == iters, eps, st);
+        const bool clean = skip_zero_ && (clean_first || it > 0);
+        rc = launch_sweeps(true, plus_appr != 0, it + 1 == iters, eps, st, clean);
         if (rc) return rc;
         rc = launch_finalize(plus_appr, minus_appr, st);
         if (rc) return rc;
@@ -478,18 +492,19 @@ int Engine::launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t
 }
 
 int Engine::run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStream_t st,
-                bool prime) {
+                bool prime, bool clean_first) {
     if (psi_mode < BLDM_PSI_EXACT || psi_mode > BLDM_PSI_LEGACY_CUDA) return BLDM_ERR_BAD_ARG;
     if (iters == 0 || insts_.empty()) return BLDM_OK;
-    if (!use_graph || st == nullptr) return launch_sequence(iters, psi_mode, eps, st, prime);
+    if (!use_graph || st == nullptr)
+        return launch_sequence(iters, psi_mode, eps, st, prime, clean_first);
     uint64_t eb;
     std::memcpy(&eb, &eps, sizeof eb);
-    const auto key = std::make_tuple(iters, psi_mode, eb, prime);
+    const auto key = std::make_tuple(iters, psi_mode, eb, prime, clean_first);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
         const uint64_t l0 = launches_;
         ENG_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        const int rc = launch_sequence(iters, psi_mode, eps, st, prime);
+        const int rc = launch_sequence(iters, psi_mode, eps, st, prime, clean_first);
         cudaGraph_t g = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(st, &g);
         launches_ = l0;

@@ -61,11 +61,13 @@ struct EngineInstance {
     unsigned* counter = nullptr;
     double* delta = nullptr;
     double* rel = nullptr;
+    int* nz_rows = nullptr;  // [n_bands][x] rows with X != 0 per band, ascending
+    int* nz_cnt = nullptr;   // [n_bands][x + 1] running counts of nz_rows
 };
 
 // Byte sizes of an instance's buffers, in the order of EngineInstance's fields.
 struct InstanceBytes {
-    size_t X, S, alpha, beta, pjk, ipk, psiB, psiA, psiAS, asum, counter, delta, rel;
+    size_t X, S, alpha, beta, pjk, ipk, psiB, psiA, psiAS, asum, counter, delta, rel, nzr, nzc;
     size_t total(size_t align) const;
 };
 
@@ -74,7 +76,10 @@ constexpr int kMinTileRows = 32;
 
 class Engine {
   public:
-    Engine(int dtype, int rows_per_tile);
+    // skip_zero: once an update of every instance has stored the zeros of its
+    // fibers with X == 0, later updates skip those fibers' stores and the rows
+    // whose band segment of X is all zero (the result is the same).
+    Engine(int dtype, int rows_per_tile, bool skip_zero = true);
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
@@ -96,6 +101,8 @@ class Engine {
     // Points the instance's buffers into `base` (InstanceBytes layout, 256-aligned).
     void bind(EngineInstance& in, void* base) const;
 
+    // Row lists of the instance's band segments with X != 0 (after X is set).
+    int set_row_lists(EngineInstance& in, cudaStream_t st) const;
     // (Re)builds the launch tables for the given instances; the pointers must
     // stay valid until the next build.  Clears the per-instance counters on st.
     int build(const std::vector<EngineInstance*>& insts, cudaStream_t st);
@@ -103,8 +110,10 @@ class Engine {
     // buffers), tracking the relative change of the last one.  With prime,
     // the run first computes the axis sums and digamma tables of the current
     // S; without, it relies on those the last update (or prime()) left.
+    // clean_first: every instance has had an update since its S was set, so
+    // even the first update of this run may skip zero rows and stores.
     int run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStream_t st,
-            bool prime = true);
+            bool prime = true, bool clean_first = false);
     // Axis sums and digamma tables of the current S of every instance.
     int prime(int psi_mode, cudaStream_t st);
     int check(cudaStream_t st);
@@ -128,8 +137,10 @@ class Engine {
         cudaStream_t stream = nullptr;
         cudaEvent_t done = nullptr;
     };
-    int launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st, bool prime);
-    int launch_sweeps(bool update, bool appr, bool track, double eps, cudaStream_t st);
+    int launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st, bool prime,
+                        bool clean_first);
+    int launch_sweeps(bool update, bool appr, bool track, double eps, cudaStream_t st,
+                      bool clean);
     int launch_finalize(int plus_appr, int minus_appr, cudaStream_t st);
     void free_tables();
     void drop_graphs();
@@ -137,6 +148,7 @@ class Engine {
     int dtype_;
     size_t es_;
     int rows_per_tile_;
+    bool skip_zero_;
     int num_sms_;
     std::vector<EngineInstance*> insts_;
     std::vector<ShapeClass> classes_;
@@ -152,7 +164,7 @@ class Engine {
     int fin_blocks_ = 0;
     cudaEvent_t fork_ = nullptr;
     uint64_t launches_ = 0;
-    std::map<std::tuple<size_t, int, uint64_t, bool>, cudaGraphExec_t> graphs_;
+    std::map<std::tuple<size_t, int, uint64_t, bool, bool>, cudaGraphExec_t> graphs_;
     std::map<ClassKey, ClassTune> tune_;
 };
 

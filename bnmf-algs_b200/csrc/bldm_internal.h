@@ -52,6 +52,9 @@ struct PlanImpl {
     double* asum_part = nullptr;  // [n_ablk][z]
     unsigned* counter = nullptr;  // finalize last-block counter
     int* err = nullptr;           // device error word
+    bool skip_zero = false;       // bldm_tuning::skip_zero_rows
+    int* nz_rows = nullptr;       // [n_bands][x] rows with X != 0 per band (skip_zero)
+    int* nz_cnt = nullptr;        // [n_bands][x + 1] running counts (skip_zero)
     uint64_t launches = 0;
 };
 

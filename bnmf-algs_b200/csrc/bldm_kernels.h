@@ -28,6 +28,11 @@ template <typename T> struct SweepInst {
     double* part_pjk;    // [n_rr][y][z]
     double* part_ipk;    // [n_bands][x][z]
     double* delta_part;  // [n_rr * n_bands][2] (sum |S_new - S|, sum |S_new|) or null
+    // Rows with some X != 0 in a band's columns, for updates that skip the
+    // others: nz_rows[b][0 .. nz_cnt[b][x]) ascending, nz_cnt[b][i] = entries
+    // of band b below row i.  null: every row is swept.
+    const int* nz_rows;  // [n_bands][x]
+    const int* nz_cnt;   // [n_bands][x + 1]
     long long x, y, z;
     int n_bands, band_w, wpr;
     int n_rr, rr_base, rr_extra;
@@ -100,14 +105,22 @@ template <typename T> struct BatchFinParams {
     int plus_appr, minus_appr;
 };
 
-// Kernel entry points by lane shape (defined in bldm_sweep.cu).
-void* pick_sweep_fn(int dtype, int vec, int lpf, int mch, bool update, bool appr, bool batch,
+// Kernel entry points by lane shape (defined in bldm_sweep.cu).  mode: 0 the
+// axis sums of S, 1 the update, 2 the compact update (rows listed in
+// SweepInst::nz_rows only, no stores of zeros: valid once an update has
+// stored them).
+enum SweepMode : int { SWEEP_SUMS = 0, SWEEP_UPDATE = 1, SWEEP_COMPACT = 2 };
+void* pick_sweep_fn(int dtype, int vec, int lpf, int mch, int mode, bool appr, bool batch,
                     bool multirow);
 void* finalize_batch_fn(int dtype);
-void* pick_sweep_f64_plain(int vec, int lpf, int mch, bool update, bool appr, bool mr);
-void* pick_sweep_f64_batch(int vec, int lpf, int mch, bool update, bool appr, bool mr);
-void* pick_sweep_f32_plain(int vec, int lpf, int mch, bool update, bool mr);
-void* pick_sweep_f32_batch(int vec, int lpf, int mch, bool update, bool mr);
+void* pick_sweep_f64_plain(int vec, int lpf, int mch, int mode, bool appr, bool mr);
+void* pick_sweep_f64_batch(int vec, int lpf, int mch, int mode, bool appr, bool mr);
+void* pick_sweep_f32_plain(int vec, int lpf, int mch, int mode, bool mr);
+void* pick_sweep_f32_batch(int vec, int lpf, int mch, int mode, bool mr);
+// Row lists of SweepInst::nz_rows / nz_cnt from X (row-major x*y, storage
+// type per dtype) for bands of band_w columns.
+int launch_nz_rows(int dtype, const void* dX, long long x, long long y, int band_w, int n_bands,
+                   int* nz_rows, int* nz_cnt, cudaStream_t st);
 int launch_init_S(int dtype, const void* dX, void* dS, long long nf, long long z, uint64_t seed,
                   cudaStream_t st);
 

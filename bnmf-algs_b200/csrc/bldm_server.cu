@@ -130,6 +130,8 @@ int bldm_server::admit(Request* r) {
         e = cudaMemcpyAsync(r->inst.beta, r->beta.data(), r->z * 8, cudaMemcpyHostToDevice,
                             stream);
     if (e != cudaSuccess) return cuda_status(e);
+    rc = eng->set_row_lists(r->inst, stream);
+    if (rc) return rc;
     return launch_init_S(eng->dtype(), r->inst.X, r->inst.S, (long long)(r->x * r->y),
                          (long long)r->z, r->seed, stream);
 }
@@ -271,8 +273,10 @@ void bldm_server::loop() {
         }
         const double host_ms = ms_between(h0, Clock::now());
         if (rc == BLDM_OK) rc = cuda_status(cudaEventRecord(ev0, stream));
+        // requests admitted this round have not had an update yet
         if (rc == BLDM_OK)
-            rc = eng->run(cfg.iters_per_round, cfg.psi_mode, cfg.eps, false, stream, false);
+            rc = eng->run(cfg.iters_per_round, cfg.psi_mode, cfg.eps, false, stream, false,
+                          fresh.empty());
         if (rc == BLDM_OK) rc = cuda_status(cudaEventRecord(ev1, stream));
         if (rc == BLDM_OK) rc = eng->check(stream);
         if (rc == BLDM_OK)

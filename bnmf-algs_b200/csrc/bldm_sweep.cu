@@ -227,18 +227,19 @@ template <typename T> using BatchSweepFn = void (*)(const BatchSweepParams<T>);
 
 // The sweep kernel for a lane shape: plain (one instance) or batch, one row
 // or several rows per stage.  The instantiations live in bldm_pick_*.cu.
-void* pick_sweep_fn(int dtype, int vec, int lpf, int mch, bool update, bool appr, bool batch,
+void* pick_sweep_fn(int dtype, int vec, int lpf, int mch, int mode, bool appr, bool batch,
                     bool multirow) {
+    if (mode < SWEEP_SUMS || mode > SWEEP_COMPACT) return nullptr;
     if (dtype == BLDM_F64)
-        return batch ? pick_sweep_f64_batch(vec, lpf, mch, update, appr, multirow)
-                     : pick_sweep_f64_plain(vec, lpf, mch, update, appr, multirow);
-    return batch ? pick_sweep_f32_batch(vec, lpf, mch, update, multirow)
-                 : pick_sweep_f32_plain(vec, lpf, mch, update, multirow);
+        return batch ? pick_sweep_f64_batch(vec, lpf, mch, mode, appr, multirow)
+                     : pick_sweep_f64_plain(vec, lpf, mch, mode, appr, multirow);
+    return batch ? pick_sweep_f32_batch(vec, lpf, mch, mode, multirow)
+                 : pick_sweep_f32_plain(vec, lpf, mch, mode, multirow);
 }
 
-template <typename T> SweepFn<T> pick_sweep(const SweepCfg& c, bool update, bool appr) {
+template <typename T> SweepFn<T> pick_sweep(const SweepCfg& c, int mode, bool appr) {
     return reinterpret_cast<SweepFn<T>>(pick_sweep_fn(sizeof(T) == 8 ? BLDM_F64 : BLDM_F32, c.vec,
-                                                      c.lpf, c.mch, update, appr, false,
+                                                      c.lpf, c.mch, mode, appr, false,
                                                       c.wpr < kSweepWarps));
 }
 
@@ -364,6 +365,11 @@ int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_
     off = align_up(off + size_t(c.n_ablk) * z * 8, a);
     const size_t o_cnt = off;
     off = align_up(off + 64, a);
+    p->skip_zero = tune && tune->skip_zero_rows != 0;
+    const size_t o_nzr = off;
+    if (p->skip_zero) off = align_up(off + size_t(c.n_bands) * x * 4, a);
+    const size_t o_nzc = off;
+    if (p->skip_zero) off = align_up(off + size_t(c.n_bands) * (x + 1) * 4, a);
     p->ws_bytes = off;
     cudaError_t e = cudaMalloc(&p->ws, p->ws_bytes);
     if (e != cudaSuccess) {
@@ -379,15 +385,17 @@ int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_
     p->asum_part = reinterpret_cast<double*>(base + o_asum);
     p->counter = reinterpret_cast<unsigned*>(base + o_cnt);
     p->err = reinterpret_cast<int*>(base + o_cnt + 16);
+    p->nz_rows = p->skip_zero ? reinterpret_cast<int*>(base + o_nzr) : nullptr;
+    p->nz_cnt = p->skip_zero ? reinterpret_cast<int*>(base + o_nzc) : nullptr;
     BLDM_CU(cudaMemset(base + o_cnt, 0, 64));
     // Opt the selected kernels into large dynamic shared memory.
-    for (int upd = 0; upd < 2; ++upd)
+    for (int mode = SWEEP_SUMS; mode <= SWEEP_COMPACT; ++mode)
         for (int ap = 0; ap < 2; ++ap) {
             void* fn = nullptr;
             if (dtype == BLDM_F64)
-                fn = reinterpret_cast<void*>(pick_sweep<double>(c, upd != 0, ap != 0));
+                fn = reinterpret_cast<void*>(pick_sweep<double>(c, mode, ap != 0));
             else
-                fn = reinterpret_cast<void*>(pick_sweep<float>(c, upd != 0, ap != 0));
+                fn = reinterpret_cast<void*>(pick_sweep<float>(c, mode, ap != 0));
             if (!fn) return BLDM_ERR_UNSUPPORTED;
             const int rc_attr = ensure_smem_attr(fn, c.smem_update);
             if (rc_attr) return rc_attr;
@@ -443,13 +451,13 @@ int plan_setup_in(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, void* ws
     p->counter = reinterpret_cast<unsigned*>(base + o_cnt);
     p->err = reinterpret_cast<int*>(base + o_cnt + 16);
     BLDM_CU(cudaMemsetAsync(base + o_cnt, 0, 64, st));
-    for (int upd = 0; upd < 2; ++upd)
+    for (int mode = SWEEP_SUMS; mode <= SWEEP_COMPACT; ++mode)
         for (int ap = 0; ap < 2; ++ap) {
             void* fn = nullptr;
             if (dtype == BLDM_F64)
-                fn = reinterpret_cast<void*>(pick_sweep<double>(c, upd != 0, ap != 0));
+                fn = reinterpret_cast<void*>(pick_sweep<double>(c, mode, ap != 0));
             else
-                fn = reinterpret_cast<void*>(pick_sweep<float>(c, upd != 0, ap != 0));
+                fn = reinterpret_cast<void*>(pick_sweep<float>(c, mode, ap != 0));
             if (!fn) return BLDM_ERR_UNSUPPORTED;
             const int rc_attr = ensure_smem_attr(fn, c.smem_update);
             if (rc_attr) return rc_attr;
@@ -475,6 +483,8 @@ static SweepParams<T> sweep_params(PlanImpl* p, const void* dX, void* dS, double
     in.part_pjk = p->part_pjk;
     in.part_ipk = p->part_ipk;
     in.delta_part = nullptr;
+    in.nz_rows = p->nz_rows;
+    in.nz_cnt = p->nz_cnt;
     in.x = (long long)p->x;
     in.y = (long long)p->y;
     in.z = (long long)p->z;
@@ -529,19 +539,28 @@ static int run_typed(PlanImpl* p, const void* dX, const double* dalpha, const do
     const SweepCfg& c = p->cfg;
     const int plus_appr = psi_mode != BLDM_PSI_EXACT;
     const int minus_appr = psi_mode == BLDM_PSI_APPR;
-    SweepFn<T> fsum = pick_sweep<T>(c, false, true);
-    SweepFn<T> fupd = pick_sweep<T>(c, true, plus_appr != 0);
-    if (!fsum || !fupd) return BLDM_ERR_UNSUPPORTED;
+    SweepFn<T> fsum = pick_sweep<T>(c, SWEEP_SUMS, true);
+    SweepFn<T> fupd = pick_sweep<T>(c, SWEEP_UPDATE, plus_appr != 0);
+    // From the second update on, the first one has stored the zeros of every
+    // fiber with X == 0: with skip_zero_rows those updates sweep listed rows.
+    SweepFn<T> flater = p->skip_zero ? pick_sweep<T>(c, SWEEP_COMPACT, plus_appr != 0) : fupd;
+    if (!fsum || !fupd || !flater) return BLDM_ERR_UNSUPPORTED;
     const SweepParams<T> sp = sweep_params<T>(p, dX, dS, eps);
     const FinParams<T> fp = fin_params<T>(p, dalpha, dbeta, plus_appr, minus_appr);
     const dim3 grid_s(unsigned(c.n_bands) * unsigned(c.n_rr));
     const dim3 grid_f(unsigned(fp.f.nbB + fp.f.n_ablk));
+    if (p->skip_zero) {
+        const int rc = launch_nz_rows(p->dtype, dX, (long long)p->x, (long long)p->y, c.band_w,
+                                      c.n_bands, p->nz_rows, p->nz_cnt, st);
+        if (rc) return rc;
+        p->launches += 2;
+    }
     fsum<<<grid_s, kSweepThreads, c.smem_sums, st>>>(sp);
     finalize_kernel<T><<<grid_f, kFinThreads, 0, st>>>(fp);
     p->launches += 2;
     for (size_t it = 0; it < max_iter; ++it) {
         if (ev && 2 * it + 1 < nev) cudaEventRecord(ev[2 * it], st);
-        fupd<<<grid_s, kSweepThreads, c.smem_update, st>>>(sp);
+        (it == 0 ? fupd : flater)<<<grid_s, kSweepThreads, c.smem_update, st>>>(sp);
         if (ev && 2 * it + 1 < nev) cudaEventRecord(ev[2 * it + 1], st);
         p->launches += 1;
         if (it + 1 < max_iter) {
@@ -577,6 +596,63 @@ int plan_init_S(PlanImpl* p, const void* dX, void* dS, uint64_t seed, cudaStream
                                                      static_cast<float*>(dS), nf,
                                                      (long long)p->z, seed);
     p->launches += 1;
+    return cuda_status(cudaGetLastError());
+}
+
+// One warp per (row, band): nz_rows[b][i] = 1 when row i has a nonzero X in
+// band b's columns (lanes read the segment coalesced).
+template <typename T>
+__global__ void nz_flags_kernel(const T* X, long long x, long long y, int band_w, int n_bands,
+                                int* flags) {
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= x * n_bands) return;  // warp-uniform
+    const long long i = w / n_bands;
+    const int b = int(w % n_bands);
+    const long long j0 = (long long)b * band_w;
+    const long long j1 = min(y, j0 + band_w);
+    bool nz = false;
+    for (long long j = j0 + lane; j < j1; j += 32) nz = nz || X[i * y + j] != T(0);
+    nz = __any_sync(0xffffffffu, nz);
+    if (lane == 0) flags[(long long)b * x + i] = nz ? 1 : 0;
+}
+
+// One warp per band: compacts the band's flags into its ascending row list in
+// place (an entry is written at or below the index it was read from, after
+// the warp's reads of that chunk) and writes the running counts.
+__global__ void nz_compact_kernel(long long x, int n_bands, int* nz_rows, int* nz_cnt) {
+    const int b = int(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= n_bands) return;  // warp-uniform
+    int* list = nz_rows + (long long)b * x;
+    int* cnt = nz_cnt + (long long)b * (x + 1);
+    int base = 0;
+    for (long long i0 = 0; i0 < x; i0 += 32) {
+        const long long i = i0 + lane;
+        const bool nz = i < x && list[i] != 0;
+        const unsigned m = __ballot_sync(0xffffffffu, nz);
+        const int pre = __popc(m & ((1u << lane) - 1u));
+        if (i < x) cnt[i] = base + pre;
+        __syncwarp();
+        if (nz) list[base + pre] = int(i);
+        __syncwarp();
+        base += __popc(m);
+    }
+    if (lane == 0) cnt[x] = base;
+}
+
+int launch_nz_rows(int dtype, const void* dX, long long x, long long y, int band_w, int n_bands,
+                   int* nz_rows, int* nz_cnt, cudaStream_t st) {
+    const long long warps = x * n_bands;
+    const unsigned blocks = unsigned((warps * 32 + 255) / 256);
+    if (dtype == BLDM_F64)
+        nz_flags_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(dX), x, y,
+                                                        band_w, n_bands, nz_rows);
+    else
+        nz_flags_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const float*>(dX), x, y,
+                                                       band_w, n_bands, nz_rows);
+    const unsigned cblocks = unsigned(((long long)n_bands * 32 + 255) / 256);
+    nz_compact_kernel<<<cblocks, 256, 0, st>>>(x, n_bands, nz_rows, nz_cnt);
     return cuda_status(cudaGetLastError());
 }
 

@@ -49,7 +49,8 @@ __device__ __forceinline__ uintptr_t align_up16(uintptr_t a) {
 // lane = g*LPF + q handles fiber slot g of its warp and elements
 // k = (m*LPF + q)*VEC + v; warp w works on row slot w / wpr and column group
 // w % wpr of the band.
-template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool BATCH, bool MULTIROW>
+template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool BATCH, bool MULTIROW,
+          bool COMPACT>
 __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLaunch& L, int band,
                                            int rr, int tile, unsigned char* smem) {
     constexpr int NW = kSweepWarps;
@@ -73,14 +74,23 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
     const int cw = (int)min((long long)in.band_w, in.y - c0);
     const long long r0 = (long long)rr * in.rr_base + min(rr, in.rr_extra);
     const int nrows = (int)min((long long)(in.rr_base + (rr < in.rr_extra ? 1 : 0)), in.x - r0);
-    const int nrounds = (nrows + RPS - 1) / RPS;
     const SlotLayout lay(in.band_w, z, int(sizeof(T)));
+    // COMPACT (an update after an earlier one has stored the zeros of every
+    // fiber with X == 0): zero passes store nothing, and with row lists only
+    // the tile's rows whose band segment of X has a nonzero are swept; the
+    // others' update is zero and their S_ipk partials are the zeros stored
+    // before.
+    static_assert(UPDATE || !COMPACT, "compact sweeps are updates");
+    const bool compact = COMPACT && in.nz_rows != nullptr;
+    constexpr bool clean = COMPACT;
 
     unsigned char* stage0 = smem;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)L.stages * L.stage_bytes);
     double* red = reinterpret_cast<double*>(bars + 8);                    // [stages][NW][z]
     T* sAS = reinterpret_cast<T*>(red + (size_t)L.stages * NW * z);         // [z]
     __shared__ int cnt[8];             // per-stage arrivals of warps (monotonic)
+    __shared__ int srow[8][8];         // compact update: row of (stage, row slot)
+    __shared__ int nzr[2];             // compact update: the tile's row-list range
     __shared__ double2 ltab[kLogTabN];  // ln table of the FP64 digamma
     __shared__ double dsum[NW][2];
 
@@ -89,11 +99,20 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         mbar_fence_init();
     }
     if (tid < 8) cnt[tid] = 0;
+    if (compact && tid == 0) {
+        const int* cb = in.nz_cnt + (long long)band * (in.x + 1);
+        nzr[0] = cb[r0];
+        nzr[1] = cb[r0 + nrows];
+    }
     if (UPDATE) {
         for (long long k = tid; k < z; k += kSweepThreads) sAS[k] = in.psiAS[k];
         if (sizeof(T) == 8 && APPR) log_tab_init(ltab, tid, kSweepThreads);
     }
     __syncthreads();
+    // entries of the row sequence: the tile's rows, or its listed rows
+    const int nlist = compact ? nzr[1] - nzr[0] : nrows;
+    const int* rowlist = compact ? in.nz_rows + (long long)band * in.x + nzr[0] : nullptr;
+    const int nrounds = (nlist + RPS - 1) / RPS;
 
     const uint64_t pol_stream = policy_evict_first();
     const uint64_t pol_keep = policy_evict_last();
@@ -106,14 +125,17 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         return st + (size_t)RPS * (lay.capS + lay.capX) + (size_t)r * lay.capA;
     };
 
-    // Round t holds rows r0 + t*RPS + r, r < RPS.
+    // Round t holds entries t*RPS + r, r < RPS, of the row sequence; a compact
+    // update records their rows in srow[stage] for the consumers (published
+    // by the stage's mbarrier arrival, read after its wait).
     auto issue = [&](int t) {
         const int s = t % L.stages;
         unsigned char* st = stage0 + (size_t)s * L.stage_bytes;
-        const int nr = min(RPS, nrows - t * RPS);
+        const int nr = min(RPS, nlist - t * RPS);
         uint32_t tot = 0;
         for (int r = 0; r < nr; ++r) {
-            const long long i = r0 + (long long)t * RPS + r;
+            const long long i = compact ? (long long)rowlist[t * RPS + r] : r0 + (long long)t * RPS + r;
+            if (compact) srow[s][r] = int(i);
             const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
             const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
             tot += uint32_t(align_up16(aS + (uintptr_t)cw * z * sizeof(T)) - align_down16(aS));
@@ -125,7 +147,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         }
         mbar_arrive_expect_tx(&bars[s], tot);
         for (int r = 0; r < nr; ++r) {
-            const long long i = r0 + (long long)t * RPS + r;
+            const long long i = compact ? (long long)srow[s][r] : r0 + (long long)t * RPS + r;
             const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
             const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
             bulk_g2s(slotS(st, r), reinterpret_cast<const void*>(align_down16(aS)),
@@ -186,8 +208,9 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             return;
         }
         unsigned char* st = stage0 + (size_t)s * L.stage_bytes;
-        const bool row_ok = t * RPS + rs < nrows;  // warp-uniform
-        const long long i = r0 + (long long)t * RPS + rs;
+        const bool row_ok = t * RPS + rs < nlist;  // warp-uniform
+        const long long i =
+            compact ? (row_ok ? (long long)srow[s][rs] : 0) : r0 + (long long)t * RPS + rs;
 
         Acc<T> ip[MCH][VEC];
 #pragma unroll
@@ -315,7 +338,8 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
 
 #pragma unroll
                 for (int c = 0; c < CPW; ++c) {
-                    if ((work >> c) & 1u) continue;
+                    // a compact update finds the zeros of these fibers stored already
+                    if (((work >> c) & 1u) || clean) continue;
                     const int jl = (cg * CPW + c) * FPW + g;
                     T zs[VEC];
 #pragma unroll
@@ -401,9 +425,9 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         if (last) {
             __threadfence_block();
             const double* reds = red + (size_t)s * NW * z;
-            const int nr = min(RPS, nrows - t * RPS);
+            const int nr = min(RPS, nlist - t * RPS);
             for (int r = 0; r < nr; ++r) {
-                const long long ir = r0 + (long long)t * RPS + r;
+                const long long ir = compact ? (long long)srow[s][r] : r0 + (long long)t * RPS + r;
                 const double* redr = reds + (size_t)r * wpr * z;
                 for (long long k = lane; k < z; k += 32) {
                     // all loads issued together; warps beyond wpr add nothing
@@ -484,23 +508,25 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
     }
 }
 
-template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool MULTIROW>
+template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool MULTIROW,
+          bool COMPACT>
 __global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(const SweepParams<T> p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int band = blockIdx.x % p.in.n_bands;
     const int rr = blockIdx.x / p.in.n_bands;
-    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR, false, MULTIROW>(p.in, p.L, band, rr,
-                                                               int(blockIdx.x), smem);
+    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR, false, MULTIROW, COMPACT>(p.in, p.L, band, rr,
+                                                                        int(blockIdx.x), smem);
 }
 
-template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool MULTIROW>
+template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool MULTIROW,
+          bool COMPACT>
 __global__ void __launch_bounds__(kSweepThreads, 2) sweep_batch_kernel(const BatchSweepParams<T> p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const BatchTile tl = p.tiles[blockIdx.x];
     SweepInst<T> in = p.insts[tl.inst];
     if (!p.track) in.delta_part = nullptr;
-    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR, true, MULTIROW>(in, p.L, tl.band, tl.rr,
-                                                              tl.rr * in.n_bands + tl.band, smem);
+    sweep_tile<T, VEC, LPF, MCH, UPDATE, APPR, true, MULTIROW, COMPACT>(
+        in, p.L, tl.band, tl.rr, tl.rr * in.n_bands + tl.band, smem);
 }
 
 

@@ -136,11 +136,18 @@ int bldm_plan_create(bldm_plan** plan, size_t x, size_t y, size_t z, int dtype);
  * resident sweep CTAs per SM (1 or 2); row_ranges: row ranges the rows of a
  * band of columns are split into (one CTA each).  The reference has no
  * counterpart (its kernels use fixed 32x32 / 16x16x4 blocks,
- * cuda_src/bld_mult/bld_mult_cuda_funcs.cu:18-24); the autotuner sets them. */
+ * cuda_src/bld_mult/bld_mult_cuda_funcs.cu:18-24); the autotuner sets them.
+ * skip_zero_rows = 1: an update maps every fiber with X == 0 to zero, so once
+ * the first update of a run has stored those zeros, the later updates neither
+ * read nor write the rows of a band whose X segment is all zero, nor store
+ * the zeros of single fibers with X == 0 again.  The result is bitwise the
+ * same; the work scales with the rows that hold nonzeros.  Off by default:
+ * the plain path streams all of S each iteration as the reference does. */
 typedef struct bldm_tuning {
     int stages;
     int ctas_per_sm;
     int row_ranges;
+    int skip_zero_rows;
 } bldm_tuning;
 int bldm_plan_create_tuned(bldm_plan** plan, size_t x, size_t y, size_t z, int dtype,
                            const bldm_tuning* tuning);

@@ -296,3 +296,33 @@ def test_kat_8x10_on_gpu(bldm, oracle, kat, is_approx, use_appr):
     assert oracle.sparseness(S) >= kat["sparseness_min"]
     assert is_approx(X, S.sum(2), kat["rowsum_isapprox_" + name])
     assert rel_err(S.reshape(-1), kat["S_" + name]) <= 1e-9
+
+
+@pytest.mark.parametrize("dtype_name", ["F64", "F32"])
+def test_zero_row_skip_gives_the_same_S(bldm, workloads, dtype_name):
+    """skip_zero_rows (later updates sweep only the rows whose band segment of
+    X has a nonzero and store no zeros again) gives bitwise the S of the
+    streaming sweep, also from an S0 with mass where X == 0."""
+    import torch
+    prob = workloads.plain_small(5)
+    X, z = prob["X"], prob["z"]
+    x, y = X.shape
+    X = X.copy()
+    X[: x // 2, :] = 0.0  # whole zero rows beside the model's scattered zeros
+    X[x // 2 + 3, :] = 0.0
+    rng = np.random.default_rng(4)
+    S0 = rng.uniform(0.1, 1.0, (x, y, z))
+    tt = torch.float64 if dtype_name == "F64" else torch.float32
+    dt = getattr(bldm, dtype_name)
+    out = []
+    for skip in (False, True):
+        plan = bldm.Plan(x, y, z, dt, skip_zero_rows=skip)
+        assert plan.tuning()["skip_zero_rows"] == skip
+        dS = torch.as_tensor(S0).to("cuda", tt)
+        plan.run(torch.as_tensor(X).to("cuda", tt), dev(prob["alpha"]), dev(prob["beta"]), dS, 30,
+                 bldm.PSI_APPR)
+        plan.check()
+        out.append(dS.cpu().numpy())
+        plan.close()
+    np.testing.assert_array_equal(out[0], out[1])
+    assert not np.any(out[1][X == 0])
