@@ -164,6 +164,10 @@ SIGNATURES = {
     "bldm_psi_f32": (ctypes.c_int, [_vp, _sz, _vp, _vp]),
     "bldm_log_marginal_S": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _sz, _sz, _dp, _dp,
                                            ctypes.c_double, ctypes.c_double, _dp, _vp]),
+    "bldm_bld_fact": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _sz, _sz, ctypes.POINTER(bldm_params),
+                                     ctypes.c_double, _vp, _vp, _vp, _vp]),
+    "bldm_bld_fact_f64": (ctypes.c_int, [_dp, _sz, _sz, _sz, ctypes.POINTER(bldm_params),
+                                         ctypes.c_double, _dp, _dp, _dp]),
     "bldm_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _sz,
                                          ctypes.POINTER(_sz), ctypes.POINTER(_sz),
                                          ctypes.POINTER(_sz), ctypes.c_int]),
@@ -357,6 +361,30 @@ class Plan:
         n = ctypes.c_uint64()
         _check(lib().bldm_plan_launch_count(self._h, ctypes.byref(n)))
         return n.value
+
+
+def bld_fact(S, params, eps=1e-50, dtype=F64, stream=None):
+    """bld::bld_fact (src/bld/bld_fact.hpp:36-80): (W x*z, H z*y, L y) from S.
+
+    S is a host array (FP64 in and out, as the reference) or a device tensor
+    (outputs are device tensors of its dtype)."""
+    x, y, z = S.shape
+    if isinstance(S, np.ndarray):
+        S = np.ascontiguousarray(S, dtype=np.float64)
+        W, H, L = np.empty((x, z)), np.empty((z, y)), np.empty(y)
+        cp = params.c_struct()
+        _check(lib().bldm_bld_fact_f64(S.ctypes.data_as(_dp), x, y, z, ctypes.byref(cp),
+                                       float(eps), W.ctypes.data_as(_dp), H.ctypes.data_as(_dp),
+                                       L.ctypes.data_as(_dp)), "bld_fact")
+        return W, H, L
+    import torch
+    W = torch.empty((x, z), dtype=S.dtype, device=S.device)
+    H = torch.empty((z, y), dtype=S.dtype, device=S.device)
+    L = torch.empty((y,), dtype=S.dtype, device=S.device)
+    cp = params.c_struct()
+    _check(lib().bldm_bld_fact(_ptr(S), dtype, x, y, z, ctypes.byref(cp), float(eps), _ptr(W),
+                               _ptr(H), _ptr(L), _stream_ptr(stream)), "bld_fact")
+    return W, H, L
 
 
 def log_marginal_S(dS, params, dtype=F64, stream=None):

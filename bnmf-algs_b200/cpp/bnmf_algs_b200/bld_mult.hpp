@@ -21,6 +21,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -85,6 +86,22 @@ template <typename Scalar, size_t N> class tensor_t {
         return o;
     }
     std::array<size_t, N> dims_;
+    std::vector<Scalar> d_;
+};
+
+// Row vector (the reference's vector_t is an Eigen row vector, src/defs.hpp:27-32).
+template <typename Scalar> class vector_t {
+  public:
+    vector_t() = default;
+    explicit vector_t(size_t n) : d_(n) {}
+    long size() const { return long(d_.size()); }
+    long cols() const { return long(d_.size()); }
+    Scalar& operator()(size_t i) { return d_[i]; }
+    const Scalar& operator()(size_t i) const { return d_[i]; }
+    Scalar* data() { return d_.data(); }
+    const Scalar* data() const { return d_.data(); }
+
+  private:
     std::vector<Scalar> d_;
 };
 
@@ -194,6 +211,43 @@ tensor_t<T, 3> bld_mult_from(const matrix_t<T>& X, const tensor_t<T, 3>& S0,
         throw std::invalid_argument("bld_mult_from: S0 shape does not match X");
     return bldm_detail::solve<T, Scalar>(X, static_cast<size_t>(S0.dimension(2)), model_params,
                                          max_iter, psi_mode, eps, S0.data(), 0, "bld_mult_from");
+}
+
+// bld::bld_fact (src/bld/bld_fact.hpp:36-80): W (x*z), H (z*y) and L (y)
+// from S, computed on the GPU (sums reduced in FP64).
+template <typename T, typename Scalar>
+std::tuple<matrix_t<T>, matrix_t<T>, vector_t<T>>
+bld_fact(const tensor_t<T, 3>& S, const alloc_model::Params<Scalar>& model_params,
+         double eps = 1e-50) {
+    const size_t x = static_cast<size_t>(S.dimension(0));
+    const size_t y = static_cast<size_t>(S.dimension(1));
+    const size_t z = static_cast<size_t>(S.dimension(2));
+    if (static_cast<size_t>(model_params.alpha.size()) != x)
+        throw std::invalid_argument("Number of alpha parameters must be equal to S.dimension(0)");
+    if (static_cast<size_t>(model_params.beta.size()) != z)
+        throw std::invalid_argument("Number of beta parameters must be equal to z");
+    const std::vector<double> alpha(model_params.alpha.data(),
+                                    model_params.alpha.data() + x);
+    const std::vector<double> beta(model_params.beta.data(), model_params.beta.data() + z);
+    bldm_params p;
+    p.a = double(model_params.a);
+    p.b = double(model_params.b);
+    p.alpha = alpha.data();
+    p.n_alpha = x;
+    p.beta = beta.data();
+    p.n_beta = z;
+    const std::vector<double> Sd(S.data(), S.data() + x * y * z);
+    std::vector<double> Wd(x * z), Hd(z * y), Ld(y);
+    bldm_detail::throw_status(
+        bldm_bld_fact_f64(Sd.data(), x, y, z, &p, eps, Wd.data(), Hd.data(), Ld.data()),
+        "bld_fact");
+    matrix_t<T> W(x, z);
+    matrix_t<T> H(z, y);
+    vector_t<T> L(y);
+    for (size_t e = 0; e < x * z; ++e) W.data()[e] = T(Wd[e]);
+    for (size_t e = 0; e < z * y; ++e) H.data()[e] = T(Hd[e]);
+    for (size_t e = 0; e < y; ++e) L.data()[e] = T(Ld[e]);
+    return std::make_tuple(W, H, L);
 }
 
 }  // namespace bld

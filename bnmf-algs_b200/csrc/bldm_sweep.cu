@@ -571,6 +571,28 @@ static int run_typed(PlanImpl* p, const void* dX, const double* dalpha, const do
     return cuda_status(cudaGetLastError());
 }
 
+// Axis-sum partials of S alone (the sums sweep): part_pjk[n_rr][y][z] and
+// part_ipk[n_bands][x][z] of the plan's workspace; no X, no digamma tables.
+int plan_sums(PlanImpl* p, const void* dS, cudaStream_t st) {
+    if (!p || !p->ws || !dS) return BLDM_ERR_BAD_ARG;
+    if (reinterpret_cast<uintptr_t>(dS) & 15) return BLDM_ERR_BAD_ARG;
+    const SweepCfg& c = p->cfg;
+    const dim3 grid_s(unsigned(c.n_bands) * unsigned(c.n_rr));
+    if (p->dtype == BLDM_F64) {
+        SweepFn<double> f = pick_sweep<double>(c, SWEEP_SUMS, true);
+        if (!f) return BLDM_ERR_UNSUPPORTED;
+        f<<<grid_s, kSweepThreads, c.smem_sums, st>>>(
+            sweep_params<double>(p, nullptr, const_cast<void*>(dS), 0.0));
+    } else {
+        SweepFn<float> f = pick_sweep<float>(c, SWEEP_SUMS, true);
+        if (!f) return BLDM_ERR_UNSUPPORTED;
+        f<<<grid_s, kSweepThreads, c.smem_sums, st>>>(
+            sweep_params<float>(p, nullptr, const_cast<void*>(dS), 0.0));
+    }
+    p->launches += 1;
+    return cuda_status(cudaGetLastError());
+}
+
 int plan_run(PlanImpl* p, const void* dX, const double* dalpha, const double* dbeta, void* dS,
              size_t max_iter, int psi_mode, double eps, cudaStream_t st, cudaEvent_t* ev,
              size_t nev) {

@@ -137,9 +137,11 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             const long long i = compact ? (long long)rowlist[t * RPS + r] : r0 + (long long)t * RPS + r;
             if (compact) srow[s][r] = int(i);
             const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
-            const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
             tot += uint32_t(align_up16(aS + (uintptr_t)cw * z * sizeof(T)) - align_down16(aS));
-            tot += uint32_t(align_up16(aX + (uintptr_t)cw * sizeof(T)) - align_down16(aX));
+            if (UPDATE) {  // the axis sums of S do not read X
+                const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
+                tot += uint32_t(align_up16(aX + (uintptr_t)cw * sizeof(T)) - align_down16(aX));
+            }
             if (UPDATE) {
                 const uintptr_t aA = reinterpret_cast<uintptr_t>(in.psiA + i * z);
                 tot += uint32_t(align_up16(aA + (uintptr_t)z * sizeof(T)) - align_down16(aA));
@@ -153,9 +155,10 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             bulk_g2s(slotS(st, r), reinterpret_cast<const void*>(align_down16(aS)),
                      uint32_t(align_up16(aS + (uintptr_t)cw * z * sizeof(T)) - align_down16(aS)),
                      &bars[s], pol_stream);
-            bulk_g2s(slotX(st, r), reinterpret_cast<const void*>(align_down16(aX)),
-                     uint32_t(align_up16(aX + (uintptr_t)cw * sizeof(T)) - align_down16(aX)),
-                     &bars[s], pol_keep);
+            if (UPDATE)
+                bulk_g2s(slotX(st, r), reinterpret_cast<const void*>(align_down16(aX)),
+                         uint32_t(align_up16(aX + (uintptr_t)cw * sizeof(T)) - align_down16(aX)),
+                         &bars[s], pol_keep);
             if (UPDATE) {
                 const uintptr_t aA = reinterpret_cast<uintptr_t>(in.psiA + i * z);
                 bulk_g2s(slotA(st, r), reinterpret_cast<const void*>(align_down16(aA)),

@@ -245,6 +245,19 @@ int bldm_log_marginal_S(const void* d_S, int dtype, size_t x, size_t y, size_t z
                         const double* alpha, const double* beta, double a,
                         double b, double* result, void* stream);
 
+/* bld::bld_fact (src/bld/bld_fact.hpp:36-80): W (x*z), H (z*y) and L (y)
+ * from a BLD solution S, W(i,k) = (alpha_i + S_i+k - 1) / (sum over i of the
+ * same + eps), H(k,j) = (beta_k + S_+jk - 1) / (sum over k of the same + eps),
+ * L(j) = (a + S_+j+ - 1) / (b + 1 + eps).  Device tensors of the storage
+ * dtype, row-major; params' alpha and beta are host arrays.  The sums are
+ * reduced in FP64.  Synchronises `stream`. */
+int bldm_bld_fact(const void* d_S, int dtype, size_t x, size_t y, size_t z,
+                  const bldm_params* params, double eps, void* d_W, void* d_H, void* d_L,
+                  void* stream);
+/* The same on host FP64 arrays (the reference's interface; copies in and out). */
+int bldm_bld_fact_f64(const double* S, size_t x, size_t y, size_t z, const bldm_params* params,
+                      double eps, double* W, double* H, double* L);
+
 /* ------------------------------------------------------------------------
  * Batched solver: many independent instances of different shapes (x, y, z
  * each) solved together.  No counterpart in the reference, which solves one

@@ -105,6 +105,55 @@ static int known_answer(const char* xpath, const char* out_legacy, const char* o
     return 0;
 }
 
+// bld_fact (src/bld/bld_fact.hpp:36-80) of a small deterministic tensor
+// against its definition evaluated here with plain loops.
+static int factorization() {
+    const size_t x = 7, y = 5, z = 3;
+    tensor_t<double, 3> S(x, y, z);
+    for (size_t i = 0; i < x; ++i)
+        for (size_t j = 0; j < y; ++j)
+            for (size_t k = 0; k < z; ++k) S(i, j, k) = double((i * 7 + j * 3 + k * 5) % 11);
+    std::vector<double> alpha(x), beta(z);
+    for (size_t i = 0; i < x; ++i) alpha[i] = 1.0 + 0.25 * double(i);
+    for (size_t k = 0; k < z; ++k) beta[k] = 0.5 + double(k);
+    alloc_model::Params<double> mp(2.0, 3.0, alpha, beta);
+    auto f = bld::bld_fact(S, mp, 1e-50);
+    const matrix_t<double>& W = std::get<0>(f);
+    const matrix_t<double>& H = std::get<1>(f);
+    const vector_t<double>& L = std::get<2>(f);
+    for (size_t k = 0; k < z; ++k) {
+        double cs = 0;
+        for (size_t i = 0; i < x; ++i) {
+            double s = 0;
+            for (size_t j = 0; j < y; ++j) s += S(i, j, k);
+            cs += alpha[i] + s - 1;
+        }
+        for (size_t i = 0; i < x; ++i) {
+            double s = 0;
+            for (size_t j = 0; j < y; ++j) s += S(i, j, k);
+            REQUIRE(std::fabs(W(i, k) - (alpha[i] + s - 1) / (cs + 1e-50)) <= 1e-12);
+        }
+    }
+    for (size_t j = 0; j < y; ++j) {
+        double cs = 0, pjp = 0;
+        for (size_t k = 0; k < z; ++k) {
+            double s = 0;
+            for (size_t i = 0; i < x; ++i) s += S(i, j, k);
+            cs += beta[k] + s - 1;
+            pjp += s;
+        }
+        for (size_t k = 0; k < z; ++k) {
+            double s = 0;
+            for (size_t i = 0; i < x; ++i) s += S(i, j, k);
+            REQUIRE(std::fabs(H(k, j) - (beta[k] + s - 1) / (cs + 1e-50)) <= 1e-12);
+        }
+        REQUIRE(std::fabs(L(j) - (2.0 + pjp - 1) / (3.0 + 1 + 1e-50)) <= 1e-12 * std::fabs(L(j)));
+    }
+    alloc_model::Params<double> bad(2.0, 3.0, std::vector<double>(x + 1, 1.0), beta);
+    REQUIRE(throws_invalid([&] { bld::bld_fact(S, bad); }));
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc != 4) {
         std::fprintf(stderr, "usage: %s kat_X.txt out_legacy.txt out_appr.txt\n", argv[0]);
@@ -113,6 +162,7 @@ int main(int argc, char** argv) {
     if (parameter_checks()) return 1;
     if (zero_matrix()) return 1;
     if (known_answer(argv[1], argv[2], argv[3])) return 1;
+    if (factorization()) return 1;
     std::printf("ok\n");
     return 0;
 }

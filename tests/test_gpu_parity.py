@@ -326,3 +326,34 @@ def test_zero_row_skip_gives_the_same_S(bldm, workloads, dtype_name):
         plan.close()
     np.testing.assert_array_equal(out[0], out[1])
     assert not np.any(out[1][X == 0])
+
+
+@pytest.mark.parametrize("dtype_name", ["F64", "F32"])
+def test_bld_fact_matches_oracle(bldm, oracle, workloads, dtype_name):
+    """bld_fact of a solved S on the device against the oracle's restatement
+    (FP64 within 1e-12; FP32 storage within 1e-5 of the FP64 oracle)."""
+    import torch
+    prob = workloads.plain_small(7)
+    X, z = prob["X"], prob["z"]
+    x, y = X.shape
+    params = bldm.Params(prob["a"], prob["b"], prob["alpha"], prob["beta"])
+    S = bldm.bld_mult(X, z, params, 20, True, S0=oracle.init_S(X, z, 3))
+    W0, H0, L0 = oracle.bld_fact(S, prob["alpha"], prob["beta"], prob["a"], prob["b"], 1e-50)
+    if dtype_name == "F64":
+        W, H, L = bldm.bld_fact(S, params)  # host FP64 path
+        tol = 1e-12
+    else:
+        dS = torch.as_tensor(S).to("cuda", torch.float32)
+        W, H, L = (t.double().cpu().numpy() for t in bldm.bld_fact(dS, params, dtype=bldm.F32))
+        tol = 1e-5
+    for a, b in ((W, W0), (H, H0), (L, L0)):
+        assert np.abs(a - b).max() <= tol * np.abs(b).max()
+    # device FP64 path on a larger shape with several row ranges and bands
+    rng = np.random.default_rng(5)
+    S2 = rng.gamma(0.3, 2.0, (300, 260, 16))
+    a2, b2 = rng.uniform(1, 2, 300), rng.uniform(1, 2, 16)
+    p2 = bldm.Params(3.0, 0.5, a2, b2)
+    Wd, Hd, Ld = (t.cpu().numpy() for t in bldm.bld_fact(dev(S2), p2))
+    Wr, Hr, Lr = oracle.bld_fact(S2, a2, b2, 3.0, 0.5, 1e-50)
+    for a, b in ((Wd, Wr), (Hd, Hr), (Ld, Lr)):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
