@@ -307,6 +307,19 @@ template <bool APPR> struct PsiPass<float, APPR> {
 
 
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start while the previous kernel of the stream finishes;
+// it waits here before touching that kernel's results.  launch_dependents lets
+// the next kernel start its own preamble.  Both are no-ops otherwise.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void grid_dep_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void grid_dep_launch() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
 // Timers, bounded waits, bulk copies.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long global_ns() {

@@ -140,6 +140,8 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
 
 template <typename T>
 __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const FinParams<T> p) {
+    grid_dep_wait();  // the sweep's partials
+    grid_dep_launch();
     finalize_block<T>(p.f, int(blockIdx.x), p.plus_appr, p.minus_appr);
 }
 
@@ -555,19 +557,36 @@ static int run_typed(PlanImpl* p, const void* dX, const double* dalpha, const do
         if (rc) return rc;
         p->launches += 2;
     }
-    fsum<<<grid_s, kSweepThreads, c.smem_sums, st>>>(sp);
-    finalize_kernel<T><<<grid_f, kFinThreads, 0, st>>>(fp);
+    // Programmatic dependent launches: each kernel may begin while the one
+    // before it drains (its preamble overlaps; it waits in grid_dep_wait()).
+    // Not across the event records of a profiling run.
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    auto launch = [&](auto fn, dim3 grid, unsigned threads, size_t smem, const auto& prm) {
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = grid;
+        lc.blockDim = dim3(threads);
+        lc.dynamicSmemBytes = smem;
+        lc.stream = st;
+        lc.attrs = ev ? nullptr : attr;
+        lc.numAttrs = ev ? 0 : 1;
+        return cudaLaunchKernelEx(&lc, fn, prm);
+    };
+    cudaError_t e = launch(fsum, grid_s, kSweepThreads, c.smem_sums, sp);
+    if (e == cudaSuccess) e = launch(finalize_kernel<T>, grid_f, kFinThreads, 0, fp);
     p->launches += 2;
-    for (size_t it = 0; it < max_iter; ++it) {
+    for (size_t it = 0; it < max_iter && e == cudaSuccess; ++it) {
         if (ev && 2 * it + 1 < nev) cudaEventRecord(ev[2 * it], st);
-        (it == 0 ? fupd : flater)<<<grid_s, kSweepThreads, c.smem_update, st>>>(sp);
+        e = launch(it == 0 ? fupd : flater, grid_s, kSweepThreads, c.smem_update, sp);
         if (ev && 2 * it + 1 < nev) cudaEventRecord(ev[2 * it + 1], st);
         p->launches += 1;
-        if (it + 1 < max_iter) {
-            finalize_kernel<T><<<grid_f, kFinThreads, 0, st>>>(fp);
+        if (e == cudaSuccess && it + 1 < max_iter) {
+            e = launch(finalize_kernel<T>, grid_f, kFinThreads, 0, fp);
             p->launches += 1;
         }
     }
+    if (e != cudaSuccess) return cuda_status(e);
     return cuda_status(cudaGetLastError());
 }
 

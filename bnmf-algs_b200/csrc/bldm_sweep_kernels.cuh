@@ -99,15 +99,16 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         mbar_fence_init();
     }
     if (tid < 8) cnt[tid] = 0;
+    if (UPDATE && sizeof(T) == 8 && APPR) log_tab_init(ltab, tid, kSweepThreads);
+    // everything below reads what the previous kernels of the stream wrote
+    grid_dep_wait();
     if (compact && tid == 0) {
         const int* cb = in.nz_cnt + (long long)band * (in.x + 1);
         nzr[0] = cb[r0];
         nzr[1] = cb[r0 + nrows];
     }
-    if (UPDATE) {
+    if (UPDATE)
         for (long long k = tid; k < z; k += kSweepThreads) sAS[k] = in.psiAS[k];
-        if (sizeof(T) == 8 && APPR) log_tab_init(ltab, tid, kSweepThreads);
-    }
     __syncthreads();
     // entries of the row sequence: the tile's rows, or its listed rows
     const int nlist = compact ? nzr[1] - nzr[0] : nrows;
