@@ -168,6 +168,12 @@ SIGNATURES = {
                                      ctypes.c_double, _vp, _vp, _vp, _vp]),
     "bldm_bld_fact_f64": (ctypes.c_int, [_dp, _sz, _sz, _sz, ctypes.POINTER(bldm_params),
                                          ctypes.c_double, _dp, _dp, _dp]),
+    "bldm_bnmf_priors": (ctypes.c_int, [_sz, _sz, _sz, ctypes.POINTER(bldm_params),
+                                        ctypes.c_uint64, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "bldm_sample_S": (ctypes.c_int, [_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_uint64, ctypes.c_int,
+                                     _vp, _vp]),
+    "bldm_sample_X": (ctypes.c_int, [_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_uint64, ctypes.c_int,
+                                     _vp, _vp]),
     "bldm_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _sz,
                                          ctypes.POINTER(_sz), ctypes.POINTER(_sz),
                                          ctypes.POINTER(_sz), ctypes.c_int]),
@@ -385,6 +391,42 @@ def bld_fact(S, params, eps=1e-50, dtype=F64, stream=None):
     _check(lib().bldm_bld_fact(_ptr(S), dtype, x, y, z, ctypes.byref(cp), float(eps), _ptr(W),
                                _ptr(H), _ptr(L), _stream_ptr(stream)), "bld_fact")
     return W, H, L
+
+
+def bnmf_priors(shape, params, seed=0, dtype=F64, stream=None):
+    """alloc_model::bnmf_priors on the device: (W x*z, H z*y, L y) torch tensors."""
+    import torch
+    x, y, z = (int(v) for v in shape)
+    tt = torch.float64 if dtype == F64 else torch.float32
+    W = torch.empty((x, z), dtype=tt, device="cuda")
+    H = torch.empty((z, y), dtype=tt, device="cuda")
+    L = torch.empty((y,), dtype=tt, device="cuda")
+    cp = params.c_struct()
+    _check(lib().bldm_bnmf_priors(x, y, z, ctypes.byref(cp), int(seed), dtype, _ptr(W), _ptr(H),
+                                  _ptr(L), _stream_ptr(stream)), "bnmf_priors")
+    return W, H, L
+
+
+def _sample(fn, W, H, L, seed, shape, stream, what):
+    import torch
+    x, z = W.shape
+    y = L.shape[0]
+    dtype = F64 if W.dtype == torch.float64 else F32
+    out = torch.empty(shape(x, y, z), dtype=W.dtype, device=W.device)
+    _check(fn(_ptr(W), _ptr(H), _ptr(L), x, y, z, int(seed), dtype, _ptr(out),
+              _stream_ptr(stream)), what)
+    return out
+
+
+def sample_S(W, H, L, seed=0, stream=None):
+    """alloc_model::sample_S on the device: S_ijk ~ Poisson(W_ik H_kj L_j)."""
+    return _sample(lib().bldm_sample_S, W, H, L, seed, lambda x, y, z: (x, y, z), stream,
+                   "sample_S")
+
+
+def sample_X(W, H, L, seed=0, stream=None):
+    """X_ij ~ Poisson(sum_k W_ik H_kj L_j) on the device."""
+    return _sample(lib().bldm_sample_X, W, H, L, seed, lambda x, y, z: (x, y), stream, "sample_X")
 
 
 def log_marginal_S(dS, params, dtype=F64, stream=None):

@@ -258,6 +258,24 @@ int bldm_bld_fact(const void* d_S, int dtype, size_t x, size_t y, size_t z,
 int bldm_bld_fact_f64(const double* S, size_t x, size_t y, size_t z, const bldm_params* params,
                       double eps, double* W, double* H, double* L);
 
+/* alloc_model::bnmf_priors (src/alloc_model/alloc_model_funcs.hpp:461-502) on
+ * the device: L_j ~ Gamma(a, scale b) (GSL's gsl_ran_gamma parameterisation,
+ * as the reference), each column of W (x*z) ~ Dirichlet(alpha), each column of
+ * H (z*y) ~ Dirichlet(beta).  Device outputs of the storage dtype; params'
+ * alpha and beta are host arrays.  The draws come from a counter-based stream
+ * of `seed` (the reference's GSL stream is not reproduced).  Synchronises
+ * `stream`. */
+int bldm_bnmf_priors(size_t x, size_t y, size_t z, const bldm_params* params, uint64_t seed,
+                     int dtype, void* d_W, void* d_H, void* d_L, void* stream);
+/* alloc_model::sample_S (alloc_model_funcs.hpp:523-552): S_ijk ~
+ * Poisson(W_ik H_kj L_j), device tensors of the storage dtype. */
+int bldm_sample_S(const void* d_W, const void* d_H, const void* d_L, size_t x, size_t y,
+                  size_t z, uint64_t seed, int dtype, void* d_S, void* stream);
+/* X_ij ~ Poisson(sum_k W_ik H_kj L_j), the distribution of sum_k S_ijk, drawn
+ * directly (no counterpart in the reference, which sums a sampled S). */
+int bldm_sample_X(const void* d_W, const void* d_H, const void* d_L, size_t x, size_t y,
+                  size_t z, uint64_t seed, int dtype, void* d_X, void* stream);
+
 /* ------------------------------------------------------------------------
  * Batched solver: many independent instances of different shapes (x, y, z
  * each) solved together.  No counterpart in the reference, which solves one
