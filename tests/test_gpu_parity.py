@@ -357,3 +357,21 @@ def test_bld_fact_matches_oracle(bldm, oracle, workloads, dtype_name):
     Wr, Hr, Lr = oracle.bld_fact(S2, a2, b2, 3.0, 0.5, 1e-50)
     for a, b in ((Wd, Wr), (Hd, Hr), (Ld, Lr)):
         assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+def test_precision_study_crop_fp64_matches_oracle(bldm, oracle, workloads):
+    """The FP64 GPU path is the reference for the FP32 precision study; it is
+    validated here against the CPU oracle on a 256x256x32 crop of that
+    workload (heavy-tailed counts, alpha, beta ~ U(0.5, 2)), all 300 iterations,
+    within 1e-9 max-norm relative.  (A 1e-15 perturbation of S0 moves this
+    crop by < 1e-10 after 300 iterations, so the bar is meaningful.)"""
+    p = workloads.precision_study(2)
+    X = np.ascontiguousarray(p["X"][:256, :256])
+    z = p["z"]
+    alpha = p["alpha"][:256]
+    oracle.set_threads(0)
+    S0 = oracle.init_S(X, z, 1)
+    ref = oracle.bld_mult(X, z, alpha, p["beta"], 300, oracle.PSI_APPR, 1e-50, S0=S0)
+    params = bldm.Params(p["a"], p["b"], alpha, p["beta"])
+    S = bldm.bld_mult(X, z, params, 300, True, S0=S0)
+    assert rel_err(S, ref) <= 1e-9

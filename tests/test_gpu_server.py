@@ -24,19 +24,21 @@ def _params(bldm, x, z):
     return bldm.Params(5.0, 0.1, np.ones(x), np.ones(z))
 
 
-def test_alone_equals_in_mix(bldm, workloads):
-    reqs = [_req(workloads, s, 10 + k) for k, s in enumerate(SHAPES)]
-    target = 2
+@pytest.mark.parametrize("target,seed", [(2, 5), (0, 17), (4, 23), (5, 31)])
+def test_alone_equals_in_mix(bldm, workloads, target, seed):
+    """A request's result is bitwise the same served alone and in a mix whose
+    other requests arrive while it is on the GPU (a handful of seeds)."""
+    reqs = [_req(workloads, s, 10 + k + seed) for k, s in enumerate(SHAPES)]
     alone = bldm.Server(dtype=bldm.F32, tol=1e-5, max_iter=200, iters_per_round=10)
     X, z = reqs[target]
-    rid = alone.submit(X, z, _params(bldm, X.shape[0], z), seed=5)
+    rid = alone.submit(X, z, _params(bldm, X.shape[0], z), seed=seed)
     assert alone.wait(rid)
     S_alone, st_alone = alone.fetch(rid)
     alone.close()
     mix = bldm.Server(dtype=bldm.F32, tol=1e-5, max_iter=200, iters_per_round=10)
     ids = {}
     for k, (X, z) in enumerate(reqs):
-        ids[k] = mix.submit(X, z, _params(bldm, X.shape[0], z), seed=5 if k == target else k)
+        ids[k] = mix.submit(X, z, _params(bldm, X.shape[0], z), seed=seed if k == target else k)
         if k == 1:
             time.sleep(0.05)  # later requests arrive while others are on the GPU
     for rid in ids.values():
@@ -121,4 +123,25 @@ def test_cancel(bldm, workloads):
     assert srv.wait(rid, 30.0)
     S, st = srv.fetch(rid)
     assert S is None and st["status"] == bldm.ERR_NOT_FOUND
+    srv.close()
+
+
+def test_fp32_served_log_marginal_vs_fp64_oracle(bldm, workloads, oracle):
+    """FP32 storage (Kahan axis sums) served to a fixed iteration count: the
+    device FP64 log-marginal of the result is within 1e-5 relative of the CPU
+    oracle's FP64 solve of the same request."""
+    srv = bldm.Server(dtype=bldm.F32, tol=0.0, max_iter=60, iters_per_round=20)
+    cases = []
+    for k, shape in enumerate([(64, 48, 8), (96, 80, 16), (40, 41, 64)]):
+        X, z = _req(workloads, shape, 50 + k)
+        p = _params(bldm, X.shape[0], z)
+        cases.append((srv.submit(X, z, p, seed=k), X, z, p, k))
+    for rid, X, z, p, k in cases:
+        assert srv.wait(rid)
+        S, st = srv.fetch(rid)
+        assert st["status"] == 0 and st["iterations"] == 60
+        ref = oracle.bld_mult(X, z, p.alpha, p.beta, 60, oracle.PSI_APPR, 1e-50,
+                              S0=oracle.init_S(X, z, k))
+        lm = oracle.log_marginal_S(ref, p.alpha, p.beta, p.a, p.b)
+        assert abs(st["log_marginal"] - lm) <= 1e-5 * abs(lm)
     srv.close()
