@@ -389,6 +389,28 @@ def run_profile(args):
     return 0
 
 
+def run_batch_probe(args):
+    """The uneven batch of --batch run for --profile-iters iterations twice,
+    without the CUDA graph (for ncu captures of the class kernels)."""
+    import torch
+    pkg = load_package()
+    import bnmf_algs_b200.workloads as W
+    shapes = W.batch_shapes(args.batch_n, 3)
+    f64 = args.dtype == "f64"
+    b = pkg.Batch(shapes, dtype=pkg.F64 if f64 else pkg.F32, rows_per_tile=args.rows_per_tile)
+    for k, (x, y, z) in enumerate(shapes):
+        pr = W.batch_instance((x, y, z), 1000 + 3 * 100003 + k)
+        b.set(k, pr["X"], pr["alpha"], pr["beta"], None, seed=k)
+    stream = torch.cuda.Stream()
+    for _ in range(2):
+        b.run(args.profile_iters, pkg.PSI_APPR, 1e-50, False, stream)
+    b.check(stream)
+    print(f"batch probe ok: {len(shapes)} instances, {b.info()['classes']} classes, "
+          f"{args.profile_iters} iterations twice")
+    b.close()
+    return 0
+
+
 def run_batch(args):
     """Batched uneven solves vs looping the plain per-instance solver."""
     import torch
@@ -709,6 +731,9 @@ def main():
                     help="batched uneven solves: 512 instances, x,y log-uniform in [32,512], "
                          "z in {4..64}, FP32, 150 iterations; vs a loop of the plain solver")
     ap.add_argument("--batch-n", type=int, default=512)
+    ap.add_argument("--batch-probe", action="store_true",
+                    help="build the --batch workload and run --profile-iters iterations twice "
+                         "without a graph (for ncu)")
     ap.add_argument("--rows-per-tile", type=int, default=0)
     ap.add_argument("--no-autotune", action="store_true",
                     help="--batch: keep the default tile height and stage depth")
@@ -728,7 +753,9 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.dtype is None:
-        args.dtype = "f32" if (args.batch or args.serve) else "f64"
+        args.dtype = "f32" if (args.batch or args.serve or args.batch_probe) else "f64"
+    if args.batch_probe:
+        return run_batch_probe(args)
     if args.profile_run:
         return run_profile(args)
     if args.kernel_matrix:
