@@ -193,6 +193,71 @@ def run_reference(args):
     return 0
 
 
+def run_sharded(args):
+    """The headline solve (1024x1024x64 FP64, 100 iterations) row-sharded over
+    the ranks: strong scaling, one NCCL all-reduce of y*z + z values per
+    iteration.  Works with one rank; it has not run on more than one GPU here."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", "29517")
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), rank=rank,
+                            world_size=world, device_id=torch.device("cuda", local))
+    pkg = load_package()
+    import bnmf_algs_b200.multi as M
+    import bnmf_algs_b200.workloads as W
+    prob = W.plain_large(1)
+    X, z, iters = prob["X"], prob["z"], prob["iters"]
+    x, y = X.shape
+    i0, i1 = M.row_shards(x, world)[rank]
+    dev = torch.device("cuda", local)
+    plan = pkg.Plan(i1 - i0, y, z, pkg.F64)
+    dX = torch.as_tensor(X[i0:i1]).to(dev)
+    da = torch.as_tensor(prob["alpha"][i0:i1]).to(dev)
+    db = torch.as_tensor(prob["beta"]).to(dev)
+    dS = torch.empty((i1 - i0, y, z), dtype=torch.float64, device=dev)
+    red = torch.empty(plan.shard_red_size(), dtype=torch.float64, device=dev)
+    sh = M.Shard(plan, dX, da, db, dS, red)
+    reduce = M.collective_allreduce(dist)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        plan.init_S(dX, dS, seed=rank)
+        M.sharded_solve([sh], iters, pkg.PSI_APPR, 1e-50, reduce)
+
+    for _ in range(args.warmup):
+        step()
+    plan.check(stream)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plan.check(stream)
+    ms = torch.tensor([e0.elapsed_time(e1) / args.steps], dtype=torch.float64, device=dev)
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_max = float(ms.item())
+    if rank == 0:
+        print(json.dumps({"metric": "S_elem_updates_per_s", "value": x * y * z * iters / (ms_max / 1e3),
+                          "unit": "S-updates/s", "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+                          "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic",
+                          "config": {"workload": "plain_1024x1024x64", "iters_per_step": iters,
+                                     "parallelism": f"row-sharded over {world} ranks",
+                                     "exchange_doubles_per_iteration": y * z + z}}))
+    plan.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_setup()
@@ -731,6 +796,8 @@ def main():
                     help="batched uneven solves: 512 instances, x,y log-uniform in [32,512], "
                          "z in {4..64}, FP32, 150 iterations; vs a loop of the plain solver")
     ap.add_argument("--batch-n", type=int, default=512)
+    ap.add_argument("--sharded", action="store_true",
+                    help="the headline solve row-sharded over the torchrun ranks (NCCL)")
     ap.add_argument("--batch-probe", action="store_true",
                     help="build the --batch workload and run --profile-iters iterations twice "
                          "without a graph (for ncu)")
@@ -756,6 +823,8 @@ def main():
         args.dtype = "f32" if (args.batch or args.serve or args.batch_probe) else "f64"
     if args.batch_probe:
         return run_batch_probe(args)
+    if args.sharded:
+        return run_sharded(args)
     if args.profile_run:
         return run_profile(args)
     if args.kernel_matrix:

@@ -152,6 +152,11 @@ SIGNATURES = {
     "bldm_plan_profile": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _sz, ctypes.c_int,
                                          ctypes.c_double, _vp, _dp, _dp]),
     "bldm_plan_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "bldm_plan_shard_red_size": (ctypes.c_int, [_vp, ctypes.POINTER(_sz)]),
+    "bldm_plan_shard_sums": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
+    "bldm_plan_shard_update": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int,
+                                              ctypes.c_double, _vp]),
+    "bldm_plan_shard_finish": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     "bldm_tensor_sums_f64": (ctypes.c_int, [_vp, _sz, _sz, _sz, _vp, _vp, _vp, _vp]),
     "bldm_update_grad_plus_f64": (ctypes.c_int, [_vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp,
                                                  _vp]),
@@ -367,6 +372,25 @@ class Plan:
         n = ctypes.c_uint64()
         _check(lib().bldm_plan_launch_count(self._h, ctypes.byref(n)))
         return n.value
+
+    # Row-sharded solve steps (see bnmf_algs_b200.multi.sharded_solve).
+    def shard_red_size(self):
+        n = ctypes.c_size_t()
+        _check(lib().bldm_plan_shard_red_size(self._h, ctypes.byref(n)))
+        return n.value
+
+    def shard_sums(self, dS, dalpha, dred, psi_mode=PSI_APPR, stream=None):
+        _check(lib().bldm_plan_shard_sums(self._h, _ptr(dS), _ptr(dalpha), _ptr(dred),
+                                          int(psi_mode), _stream_ptr(stream)), "shard_sums")
+
+    def shard_update(self, dX, dS, dalpha, dred, psi_mode=PSI_APPR, eps=1e-50, stream=None):
+        _check(lib().bldm_plan_shard_update(self._h, _ptr(dX), _ptr(dS), _ptr(dalpha),
+                                            _ptr(dred), int(psi_mode), float(eps),
+                                            _stream_ptr(stream)), "shard_update")
+
+    def shard_finish(self, dbeta, dred, psi_mode=PSI_APPR, stream=None):
+        _check(lib().bldm_plan_shard_finish(self._h, _ptr(dbeta), _ptr(dred), int(psi_mode),
+                                            _stream_ptr(stream)), "shard_finish")
 
 
 def bld_fact(S, params, eps=1e-50, dtype=F64, stream=None):

@@ -326,6 +326,33 @@ int bldm_plan_profile(bldm_plan* plan, const void* d_X, const double* d_alpha,
     return rc;
 }
 
+int bldm_plan_shard_red_size(const bldm_plan* plan, size_t* n_doubles) {
+    if (!plan || !n_doubles) return BLDM_ERR_BAD_ARG;
+    *n_doubles = plan->impl.y * plan->impl.z + plan->impl.z;
+    return BLDM_OK;
+}
+
+int bldm_plan_shard_sums(bldm_plan* plan, const void* d_S, const double* d_alpha, double* d_red,
+                         int psi_mode, void* stream) {
+    if (!plan) return BLDM_ERR_BAD_ARG;
+    return plan_shard_step(&plan->impl, nullptr, const_cast<void*>(d_S), d_alpha, d_red, false,
+                           psi_mode, 0.0, static_cast<cudaStream_t>(stream));
+}
+
+int bldm_plan_shard_update(bldm_plan* plan, const void* d_X, void* d_S, const double* d_alpha,
+                           double* d_red, int psi_mode, double eps, void* stream) {
+    if (!plan) return BLDM_ERR_BAD_ARG;
+    return plan_shard_step(&plan->impl, d_X, d_S, d_alpha, d_red, true, psi_mode, eps,
+                           static_cast<cudaStream_t>(stream));
+}
+
+int bldm_plan_shard_finish(bldm_plan* plan, const double* d_beta, const double* d_red,
+                           int psi_mode, void* stream) {
+    if (!plan) return BLDM_ERR_BAD_ARG;
+    return plan_shard_finish(&plan->impl, d_beta, d_red, psi_mode,
+                             static_cast<cudaStream_t>(stream));
+}
+
 int bldm_plan_launch_count(const bldm_plan* plan, uint64_t* count) {
     if (!plan || !count) return BLDM_ERR_BAD_ARG;
     *count = plan->impl.launches;

@@ -220,6 +220,7 @@ static void fill_tables(const std::vector<EngineInstance*>& insts, std::vector<c
         s.rr_base = c.rr_base;
         s.rr_extra = c.rr_extra;
         FinInst<T>& f = fi[n];
+        f.red = nullptr;
         f.part_pjk = in.part_pjk;
         f.part_ipk = in.part_ipk;
         f.alpha = in.alpha;

@@ -67,6 +67,10 @@ int plan_run(PlanImpl* p, const void* dX, const double* dalpha, const double* db
              cudaEvent_t* kernel_events, size_t n_kernel_events);
 int plan_init_S(PlanImpl* p, const void* dX, void* dS, uint64_t seed, cudaStream_t st);
 int plan_sums(PlanImpl* p, const void* dS, cudaStream_t st);
+int plan_shard_step(PlanImpl* p, const void* dX, void* dS, const double* dalpha, double* d_red,
+                    bool update, int psi_mode, double eps, cudaStream_t st);
+int plan_shard_finish(PlanImpl* p, const double* dbeta, const double* d_red, int psi_mode,
+                      cudaStream_t st);
 int plan_check(PlanImpl* p, cudaStream_t st);
 
 int cuda_status(cudaError_t e);

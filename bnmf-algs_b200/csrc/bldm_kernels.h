@@ -89,6 +89,11 @@ template <typename T> struct FinInst {
     unsigned* counter;
     const double* delta_part;  // [n_tiles][2] or null
     double* rel_change;        // sum |S_new - S| / sum |S_new| of the last sweep
+    // Row-sharded solves: red[y*z + z] receives this shard's S_+jk and
+    // sum_i alpha_eph(i,k) instead of the digamma tables of those shared sums
+    // (psi(alpha_eph) of the shard's own rows is still tabulated); null: the
+    // whole instance is here.
+    double* red;
     long long x, y, z;
     int n_rr, n_bands, nbB, n_ablk, rows_per_ablk, n_tiles;
 };

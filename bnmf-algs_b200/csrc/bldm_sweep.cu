@@ -70,7 +70,10 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
         if (idx < p.y * z) {
             const long long k = idx % z;
             const double s = sum_strided<false>(p.part_pjk + idx, p.y * z, p.n_rr);
-            p.psiB[idx] = T(psi_mode_f64(s + p.beta[k], plus_appr != 0));
+            if (p.red)
+                p.red[idx] = s;
+            else
+                p.psiB[idx] = T(psi_mode_f64(s + p.beta[k], plus_appr != 0));
         }
         return;
     }
@@ -118,7 +121,10 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
         for (long long k = tid; k < z; k += kFinThreads) {
             double a = 0.0;
             for (int r = 0; r < R; ++r) a += acc[r * z + k];
-            p.psiAS[k] = T(psi_mode_f64(a, minus_appr != 0));
+            if (p.red)
+                p.red[p.y * z + k] = a;
+            else
+                p.psiAS[k] = T(psi_mode_f64(a, minus_appr != 0));
         }
         if (p.delta_part && tid < 32) {
             // lanes take tiles t = lane, lane + 32, ...; then a fixed-order tree
@@ -143,6 +149,17 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const FinParams<T
     grid_dep_wait();  // the sweep's partials
     grid_dep_launch();
     finalize_block<T>(p.f, int(blockIdx.x), p.plus_appr, p.minus_appr);
+}
+
+// Row-sharded solves: the digamma tables of the shared sums once every shard's
+// red has been summed over the shards (red = [S_+jk (y*z) | sum alpha_eph (z)]).
+template <typename T>
+__global__ void __launch_bounds__(kFinThreads)
+    shard_finish_kernel(const double* red, const double* beta, long long y, long long z,
+                        T* psiB, T* psiAS, int plus_appr, int minus_appr) {
+    const long long idx = (long long)blockIdx.x * kFinThreads + threadIdx.x;
+    if (idx < y * z) psiB[idx] = T(psi_mode_f64(red[idx] + beta[idx % z], plus_appr != 0));
+    if (idx < z) psiAS[idx] = T(psi_mode_f64(red[y * z + idx], minus_appr != 0));
 }
 
 template <typename T>
@@ -520,6 +537,7 @@ static FinParams<T> fin_params(PlanImpl* p, const double* dalpha, const double* 
     f.counter = p->counter;
     f.delta_part = nullptr;
     f.rel_change = nullptr;
+    f.red = nullptr;
     f.x = (long long)p->x;
     f.y = (long long)p->y;
     f.z = (long long)p->z;
@@ -608,6 +626,62 @@ int plan_sums(PlanImpl* p, const void* dS, cudaStream_t st) {
         f<<<grid_s, kSweepThreads, c.smem_sums, st>>>(
             sweep_params<float>(p, nullptr, const_cast<void*>(dS), 0.0));
     }
+    p->launches += 1;
+    return cuda_status(cudaGetLastError());
+}
+
+// Row-sharded solves (one plan per shard of rows): a sweep of the shard (the
+// axis sums of S, or an update) followed by the finalize's reduction of the
+// shard's partials into red; shard_finish tabulates the shared digamma
+// values from red once it holds the sum over all shards.
+template <typename T>
+static int shard_step_typed(PlanImpl* p, const void* dX, void* dS, const double* dalpha,
+                            double* d_red, bool update, int psi_mode, double eps,
+                            cudaStream_t st) {
+    const SweepCfg& c = p->cfg;
+    const int plus_appr = psi_mode != BLDM_PSI_EXACT;
+    const int minus_appr = psi_mode == BLDM_PSI_APPR;
+    SweepFn<T> f = pick_sweep<T>(c, update ? SWEEP_UPDATE : SWEEP_SUMS,
+                                 update ? plus_appr != 0 : true);
+    if (!f) return BLDM_ERR_UNSUPPORTED;
+    const SweepParams<T> sp = sweep_params<T>(p, dX, dS, eps);
+    FinParams<T> fp = fin_params<T>(p, dalpha, nullptr, plus_appr, minus_appr);
+    fp.f.red = d_red;
+    const dim3 grid_s(unsigned(c.n_bands) * unsigned(c.n_rr));
+    const dim3 grid_f(unsigned(fp.f.nbB + fp.f.n_ablk));
+    f<<<grid_s, kSweepThreads, update ? c.smem_update : c.smem_sums, st>>>(sp);
+    finalize_kernel<T><<<grid_f, kFinThreads, 0, st>>>(fp);
+    p->launches += 2;
+    return cuda_status(cudaGetLastError());
+}
+
+int plan_shard_step(PlanImpl* p, const void* dX, void* dS, const double* dalpha, double* d_red,
+                    bool update, int psi_mode, double eps, cudaStream_t st) {
+    if (!p || !p->ws || !dS || !dalpha || !d_red || (update && !dX)) return BLDM_ERR_BAD_ARG;
+    if (psi_mode < 0 || psi_mode > 2) return BLDM_ERR_BAD_ARG;
+    if ((reinterpret_cast<uintptr_t>(dX) | reinterpret_cast<uintptr_t>(dS)) & 15)
+        return BLDM_ERR_BAD_ARG;
+    return p->dtype == BLDM_F64
+               ? shard_step_typed<double>(p, dX, dS, dalpha, d_red, update, psi_mode, eps, st)
+               : shard_step_typed<float>(p, dX, dS, dalpha, d_red, update, psi_mode, eps, st);
+}
+
+int plan_shard_finish(PlanImpl* p, const double* dbeta, const double* d_red, int psi_mode,
+                      cudaStream_t st) {
+    if (!p || !p->ws || !dbeta || !d_red) return BLDM_ERR_BAD_ARG;
+    if (psi_mode < 0 || psi_mode > 2) return BLDM_ERR_BAD_ARG;
+    const long long y = (long long)p->y, z = (long long)p->z;
+    const unsigned blocks = unsigned((std::max(y * z, z) + kFinThreads - 1) / kFinThreads);
+    const int plus_appr = psi_mode != BLDM_PSI_EXACT;
+    const int minus_appr = psi_mode == BLDM_PSI_APPR;
+    if (p->dtype == BLDM_F64)
+        shard_finish_kernel<double><<<blocks, kFinThreads, 0, st>>>(
+            d_red, dbeta, y, z, static_cast<double*>(p->psiB), static_cast<double*>(p->psiAS),
+            plus_appr, minus_appr);
+    else
+        shard_finish_kernel<float><<<blocks, kFinThreads, 0, st>>>(
+            d_red, dbeta, y, z, static_cast<float*>(p->psiB), static_cast<float*>(p->psiAS),
+            plus_appr, minus_appr);
     p->launches += 1;
     return cuda_status(cudaGetLastError());
 }

@@ -49,3 +49,68 @@ def aggregate_throughput(units, seconds, dist=None, device=None):
     total = sum_over_ranks(units, dist, device)
     slowest = max_over_ranks(seconds, dist, device)
     return total / slowest
+
+
+def row_shards(x, world):
+    """[i0, i1) of every rank for a row-sharded solve: contiguous blocks whose
+    sizes differ by at most one row."""
+    if world < 1 or x < world:
+        raise ValueError("need at least one row per shard")
+    base, extra = divmod(x, world)
+    out, i0 = [], 0
+    for r in range(world):
+        i1 = i0 + base + (1 if r < extra else 0)
+        out.append((i0, i1))
+        i0 = i1
+    return out
+
+
+class Shard:
+    """One row block of a sharded instance: its plan (or any object with the
+    plan's shard_* methods) and its device buffers.  red holds
+    plan.shard_red_size() FP64 values."""
+
+    def __init__(self, plan, dX, dalpha, dbeta, dS, red):
+        self.plan, self.dX, self.dalpha, self.dbeta, self.dS, self.red = (
+            plan, dX, dalpha, dbeta, dS, red)
+
+
+def sharded_solve(shards, iters, psi_mode, eps, allreduce):
+    """bld_mult over row shards.  Only the sums over rows cross shards (S_+jk
+    and sum_i alpha_eph, y*z + z values per iteration): every shard sweeps
+    its rows into its red, allreduce(reds) sums the reds of all shards of the
+    job in place (one all-reduce per iteration across ranks; a sum over the
+    list for several shards in one process), and every shard tabulates the
+    shared digamma values from the global sums.  Every rank takes the same
+    collective steps in the same order."""
+    reds = [sh.red for sh in shards]
+    for sh in shards:
+        sh.plan.shard_sums(sh.dS, sh.dalpha, sh.red, psi_mode)
+    allreduce(reds)
+    for sh in shards:
+        sh.plan.shard_finish(sh.dbeta, sh.red, psi_mode)
+    for it in range(iters):
+        for sh in shards:
+            sh.plan.shard_update(sh.dX, sh.dS, sh.dalpha, sh.red, psi_mode, eps)
+        allreduce(reds)
+        if it + 1 < iters:
+            for sh in shards:
+                sh.plan.shard_finish(sh.dbeta, sh.red, psi_mode)
+
+
+def collective_allreduce(dist):
+    """allreduce for sharded_solve with one shard per rank (NCCL or gloo)."""
+    def reduce(reds):
+        for r in reds:
+            dist.all_reduce(r, op=dist.ReduceOp.SUM)
+    return reduce
+
+
+def local_allreduce(reds):
+    """allreduce for several shards in one process: the sum in shard order,
+    written back to every shard's buffer."""
+    total = reds[0].clone()
+    for r in reds[1:]:
+        total += r
+    for r in reds:
+        r.copy_(total)

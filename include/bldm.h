@@ -193,6 +193,25 @@ int bldm_plan_profile(bldm_plan* plan, const void* d_X, const double* d_alpha,
 /* Kernels launched by the plan since creation. */
 int bldm_plan_launch_count(const bldm_plan* plan, uint64_t* count);
 
+/* Row-sharded solve (for one instance larger than a GPU's memory): shard g
+ * of G holds rows [i0, i1) of X, S and alpha in a plan of (i1-i0) x y x z.
+ * Only the sums over rows cross shards: S_+jk (y*z) and sum_i alpha_eph(i,k)
+ * (z), packed in a device buffer `red` of bldm_plan_shard_red_size doubles.
+ * One iteration: bldm_plan_shard_update (the shard's update sweep; red gets
+ * the shard's sums), an in-place sum of red over the shards (an all-reduce,
+ * e.g. NCCL), bldm_plan_shard_finish (the digamma tables from the global
+ * sums).  Start with bldm_plan_shard_sums (the sums of the initial S), the
+ * all-reduce and bldm_plan_shard_finish.  With one shard the iterations are
+ * bitwise those of bldm_plan_run.  The reference has no sharded solver; the
+ * exchange step is the one its CUDA driver performs on the host
+ * (src/bld/bld_mult/bld_mult.hpp:289-312) over the whole tensor. */
+int bldm_plan_shard_red_size(const bldm_plan* plan, size_t* n_doubles);
+int bldm_plan_shard_sums(bldm_plan* plan, const void* d_S, const double* d_alpha, double* d_red,
+                         int psi_mode, void* stream);
+int bldm_plan_shard_update(bldm_plan* plan, const void* d_X, void* d_S, const double* d_alpha,
+                           double* d_red, int psi_mode, double eps, void* stream);
+int bldm_plan_shard_finish(bldm_plan* plan, const double* d_beta, const double* d_red,
+                           int psi_mode, void* stream);
 /* ------------------------------------------------------------------------
  * Per-stage device functions.  Each mirrors one function of the reference's
  * CUDA host side so that every formula can be checked against the CPU

@@ -375,3 +375,38 @@ def test_precision_study_crop_fp64_matches_oracle(bldm, oracle, workloads):
     params = bldm.Params(p["a"], p["b"], alpha, p["beta"])
     S = bldm.bld_mult(X, z, params, 300, True, S0=S0)
     assert rel_err(S, ref) <= 1e-9
+
+
+@pytest.mark.parametrize("n_shards", [1, 3])
+def test_row_sharded_solve_matches_plan(bldm, workloads, oracle, n_shards):
+    """The row-sharded solve (bnmf_algs_b200.multi.sharded_solve over the plan's
+    shard steps), emulated with several shards in one process on one GPU:
+    one shard is bitwise the plan's solve; three shards agree to 1e-12 (the
+    sums over rows are grouped by shard) and with the CPU oracle."""
+    import torch
+    import bnmf_algs_b200.multi as M
+    prob = workloads.plain_small(9)
+    X, z = prob["X"], prob["z"]
+    x, y = X.shape
+    S0 = oracle.init_S(X, z, 4)
+    iters = 25
+    full = bldm.Plan(x, y, z)
+    dS_full = dev(S0)
+    full.run(dev(X), dev(prob["alpha"]), dev(prob["beta"]), dS_full, iters, bldm.PSI_APPR)
+    full.check()
+    shards = []
+    for i0, i1 in M.row_shards(x, n_shards):
+        plan = bldm.Plan(i1 - i0, y, z)
+        red = torch.empty(plan.shard_red_size(), dtype=torch.float64, device="cuda")
+        shards.append(M.Shard(plan, dev(X[i0:i1]), dev(prob["alpha"][i0:i1]), dev(prob["beta"]),
+                              dev(S0[i0:i1]), red))
+    M.sharded_solve(shards, iters, bldm.PSI_APPR, 1e-50, M.local_allreduce)
+    for sh in shards:
+        sh.plan.check()
+    S = np.concatenate([host(sh.dS) for sh in shards], axis=0)
+    if n_shards == 1:
+        np.testing.assert_array_equal(S, host(dS_full))
+    else:
+        assert rel_err(S, host(dS_full)) <= 1e-12
+    ref = oracle.bld_mult(X, z, prob["alpha"], prob["beta"], iters, oracle.PSI_APPR, 1e-50, S0=S0)
+    assert rel_err(S, ref) <= 1e-9
