@@ -4,8 +4,10 @@
 #include <cmath>
 #include <cstring>
 #include <list>
+#include <map>
 #include <memory>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "bldm_internal.h"
@@ -39,7 +41,16 @@ struct CacheEntry {
     double* dbeta = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // The iterations of a solve captured once per (max_iter, psi_mode, eps)
+    // and replayed: the entry's buffers are fixed, so are the launches.
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t launches = 0;
+    };
+    std::map<std::tuple<size_t, int, uint64_t>, Graph> graphs;
     ~CacheEntry() {
+        for (auto& g : graphs)
+            if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -130,6 +141,46 @@ int check_params(size_t x, size_t z, const bldm_params* p, int psi_mode) {
     return BLDM_OK;
 }
 
+// plan_run on the entry's buffers, from a CUDA graph captured on first use.
+// A capture that fails (e.g. inside a caller's own capture) falls back to
+// launching directly.
+int run_iterations(CacheEntry* e, size_t max_iter, int psi_mode, double eps) {
+    cudaStream_t st = e->stream;
+    if (max_iter == 0) return BLDM_OK;
+    uint64_t eb;
+    std::memcpy(&eb, &eps, sizeof eb);
+    const auto key = std::make_tuple(max_iter, psi_mode, eb);
+    auto it = e->graphs.find(key);
+    if (it == e->graphs.end()) {
+        CacheEntry::Graph g;
+        const uint64_t l0 = e->plan.launches;
+        cudaGraph_t graph = nullptr;
+        int r = BLDM_ERR_CUDA;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            r = plan_run(&e->plan, e->dX, e->dalpha, e->dbeta, e->dS, max_iter, psi_mode, eps,
+                         st, nullptr, 0);
+            const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+            if (r == BLDM_OK && (ce != cudaSuccess ||
+                                 cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess))
+                r = BLDM_ERR_CUDA;
+            if (graph) cudaGraphDestroy(graph);
+        }
+        g.launches = e->plan.launches - l0;
+        e->plan.launches = l0;
+        if (r != BLDM_OK || !g.exec) {
+            (void)cudaGetLastError();  // a failed capture leaves no sticky error
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            return plan_run(&e->plan, e->dX, e->dalpha, e->dbeta, e->dS, max_iter, psi_mode, eps,
+                            st, nullptr, 0);
+        }
+        it = e->graphs.emplace(key, g).first;
+    }
+    const cudaError_t le = cudaGraphLaunch(it->second.exec, st);
+    if (le != cudaSuccess) return cuda_status(le);
+    e->plan.launches += it->second.launches;
+    return BLDM_OK;
+}
+
 template <typename T>
 int solve_impl(const T* X, size_t x, size_t y, size_t z, const bldm_params* params,
                size_t max_iter, int psi_mode, double eps, const T* S0, uint64_t seed, T* S_out,
@@ -167,8 +218,7 @@ int solve_impl(const T* X, size_t x, size_t y, size_t z, const bldm_params* para
             if (r) return r;
         }
         BLDM_CU_RET(cudaEventRecord(e->ev0, st));
-        int r = plan_run(&e->plan, e->dX, e->dalpha, e->dbeta, e->dS, max_iter, psi_mode, eps, st,
-                         nullptr, 0);
+        int r = run_iterations(e, max_iter, psi_mode, eps);
         if (r) return r;
         BLDM_CU_RET(cudaEventRecord(e->ev1, st));
         BLDM_CU_RET(cudaMemcpyAsync(S_out, e->dS, x * y * z * sizeof(T), cudaMemcpyDeviceToHost,
