@@ -174,23 +174,14 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         for (int t = 0; t < n0; ++t) issue(t);
     }
 
-    // Per-lane constants for the band: psi(beta_eph) of the lane's fibers.
-    T pB[CPW][MCH][VEC];
+    // S_pjk accumulators of the lane's fibers over the tile's rows.
     Acc<T> pj[CPW][MCH][VEC];
 #pragma unroll
-    for (int c = 0; c < CPW; ++c) {
-        const int jl = (cg * CPW + c) * FPW + g;
+    for (int c = 0; c < CPW; ++c)
 #pragma unroll
-        for (int m = 0; m < MCH; ++m) {
+        for (int m = 0; m < MCH; ++m)
 #pragma unroll
-            for (int v = 0; v < VEC; ++v) {
-                const long long k = (long long)(m * LPF + q) * VEC + v;
-                pj[c][m][v].init();
-                if (UPDATE)
-                    pB[c][m][v] = (jl < cw && k < z) ? in.psiB[(c0 + jl) * z + k] : T(0);
-            }
-        }
-    }
+            for (int v = 0; v < VEC; ++v) pj[c][m][v].init();
     // only multi-instance sweeps track the relative change
     const bool track = BATCH && UPDATE && in.delta_part != nullptr;
     double d_abs = 0.0, d_new = 0.0;
@@ -371,11 +362,22 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
 #pragma unroll
                             for (int m = 0; m < MCH; ++m)
 #pragma unroll
-                                for (int v = 0; v < VEC; ++v) {
-                                    se[m][v] = sv[cc][m][v];
-                                    be[m][v] = pB[cc][m][v];
-                                }
+                                for (int v = 0; v < VEC; ++v) se[m][v] = sv[cc][m][v];
                         }
+                    }
+                    {
+                        // psi(beta_eph) of the pass's fibers through the read-only
+                        // cache (the band's slice stays in L1 over the tile); kept
+                        // out of registers, which the digamma arithmetic needs more
+                        const int jl = (cg * CPW + c) * FPW + g;
+#pragma unroll
+                        for (int m = 0; m < MCH; ++m)
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) {
+                                const long long k = (long long)(m * LPF + q) * VEC + v;
+                                be[m][v] = (jl < cw && k < z) ? __ldg(in.psiB + (c0 + jl) * z + k)
+                                                              : T(0);
+                            }
                     }
                     T sn[MCH][VEC];
                     pass_math(se, be, xe, sn);
