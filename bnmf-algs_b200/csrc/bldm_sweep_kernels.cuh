@@ -230,33 +230,38 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                         gm[m][v] = (k < z) ? sAS[k] - sA[k] : T(0);
                     }
             }
+            // The fiber values of pass c from the stage.  VEC > 1 only when
+            // z*sizeof(T) is a multiple of 16, so a chunk is entirely inside or
+            // entirely outside the fiber.
+            auto load_pass = [&](const int c, T (&se)[MCH][VEC]) {
+                const int jl = (cg * CPW + c) * FPW + g;
+#pragma unroll
+                for (int m = 0; m < MCH; ++m) {
+                    const long long k0 = (long long)(m * LPF + q) * VEC;
+                    if (jl < cw && k0 < z) {
+                        VecIO<T, VEC>::load(sS + (long long)jl * z + k0, se[m]);
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < VEC; ++v) se[m][v] = T(0);
+                    }
+                }
+            };
+            // An update reads a pass's fibers when it needs them (they stay in
+            // the stage until this warp's arrival); the sums read them all.
             T sv[CPW][MCH][VEC];
             T xv[CPW];
 #pragma unroll
             for (int c = 0; c < CPW; ++c) {
                 const int jl = (cg * CPW + c) * FPW + g;
-                const bool fv = jl < cw;
-#pragma unroll
-                for (int m = 0; m < MCH; ++m) {
-                    const long long k0 = (long long)(m * LPF + q) * VEC;
-                    // VEC > 1 only when z*sizeof(T) is a multiple of 16, so a
-                    // chunk is entirely inside or entirely outside the fiber.
-                    if (fv && k0 < z) {
-                        VecIO<T, VEC>::load(sS + (long long)jl * z + k0, sv[c][m]);
-                    } else {
-#pragma unroll
-                        for (int v = 0; v < VEC; ++v) sv[c][m][v] = T(0);
-                    }
-                }
-                xv[c] = (UPDATE && fv) ? sX[jl] : T(0);
+                if (!UPDATE) load_pass(c, sv[c]);
+                xv[c] = (UPDATE && jl < cw) ? sX[jl] : T(0);
             }
             if (UPDATE) {
                 const T teps = T(L.eps);
                 // A fiber with X == 0 updates to zero whatever its digamma values
                 // (the reference formula multiplies by X/(S_ijp+eps)).  Passes
                 // whose fibers all have X == 0 only store zeros; the others form
-                // a warp-uniform work list that runs one copy of the arithmetic,
-                // gathering the pass's operands by selects.
+                // a warp-uniform work list that runs one copy of the arithmetic.
                 unsigned work = 0;
 #pragma unroll
                 for (int c = 0; c < CPW; ++c)
@@ -339,11 +344,13 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                     T zs[VEC];
 #pragma unroll
                     for (int v = 0; v < VEC; ++v) zs[v] = T(0);
+                    T so[MCH][VEC];
+                    if (track) load_pass(c, so);
 #pragma unroll
                     for (int m = 0; m < MCH; ++m) {
                         if (track) {
 #pragma unroll
-                            for (int v = 0; v < VEC; ++v) d_abs += fabs(double(sv[c][m][v]));
+                            for (int v = 0; v < VEC; ++v) d_abs += fabs(double(so[m][v]));
                         }
                         const long long k0 = (long long)(m * LPF + q) * VEC;
                         if (jl < cw && k0 < z)
@@ -356,15 +363,9 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                     work &= work - 1;
                     T se[MCH][VEC], be[MCH][VEC], xe = T(0);
 #pragma unroll
-                    for (int cc = 0; cc < CPW; ++cc) {
-                        if (cc == c) {
-                            xe = xv[cc];
-#pragma unroll
-                            for (int m = 0; m < MCH; ++m)
-#pragma unroll
-                                for (int v = 0; v < VEC; ++v) se[m][v] = sv[cc][m][v];
-                        }
-                    }
+                    for (int cc = 0; cc < CPW; ++cc)
+                        if (cc == c) xe = xv[cc];
+                    load_pass(c, se);
                     {
                         // psi(beta_eph) of the pass's fibers through the read-only
                         // cache (the band's slice stays in L1 over the tile); kept
