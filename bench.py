@@ -445,12 +445,13 @@ def run_profile(args):
     dalpha = torch.ones(x, dtype=torch.float64, device="cuda")
     dbeta = torch.ones(z, dtype=torch.float64, device="cuda")
     dS = torch.empty((x, y, z), dtype=dt_t, device="cuda")
-    plan = pkg.Plan(x, y, z, pkg.F64 if f64 else pkg.F32)
+    plan = pkg.Plan(x, y, z, pkg.F64 if f64 else pkg.F32, skip_zero_rows=args.skip_zero_rows)
     plan.init_S(dX, dS, seed=0)
     plan.run(dX, dalpha, dbeta, dS, args.profile_iters, pkg.PSI_APPR, 1e-50)
     plan.check()
     plan.close()
-    print(f"profile run ok: {x}x{y}x{z} {args.dtype}, {args.profile_iters} iterations")
+    print(f"profile run ok: {x}x{y}x{z} {args.dtype}, {args.profile_iters} iterations"
+          f"{' (skip_zero_rows)' if args.skip_zero_rows else ''}")
     return 0
 
 
@@ -788,6 +789,8 @@ def main():
                     help="untimed: set up the workload, run --profile-iters iterations, exit "
                          "(the command profiled by ncu)")
     ap.add_argument("--profile-iters", type=int, default=3)
+    ap.add_argument("--skip-zero-rows", action="store_true",
+                    help="--profile-run: the plan option skip_zero_rows")
     ap.add_argument("--x-kind", choices=["model", "dense", "zeros"], default="model",
                     help="X of --profile-run: the plain workload's draw, 1+Poisson(10), or zeros")
     ap.add_argument("--shape", default="1024x1024x64",

@@ -218,10 +218,13 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             const uintptr_t aX = reinterpret_cast<uintptr_t>(in.X + i * in.y + c0);
             const T* sS = reinterpret_cast<const T*>(slotS(st, rs) + (aS & 15));
             const T* sX = reinterpret_cast<const T*>(slotX(st, rs) + (aX & 15));
-            T gm[MCH][VEC];
+            // grad_minus of the row's k from the stage's psi(alpha_eph) row
+            const T* sA = nullptr;
             if (UPDATE) {
                 const uintptr_t aA = reinterpret_cast<uintptr_t>(in.psiA + i * z);
-                const T* sA = reinterpret_cast<const T*>(slotA(st, rs) + (aA & 15));
+                sA = reinterpret_cast<const T*>(slotA(st, rs) + (aA & 15));
+            }
+            auto load_gm = [&](T (&gm)[MCH][VEC]) {
 #pragma unroll
                 for (int m = 0; m < MCH; ++m)
 #pragma unroll
@@ -229,7 +232,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                         const long long k = (long long)(m * LPF + q) * VEC + v;
                         gm[m][v] = (k < z) ? sAS[k] - sA[k] : T(0);
                     }
-            }
+            };
             // The fiber values of pass c from the stage.  VEC > 1 only when
             // z*sizeof(T) is a multiple of 16, so a chunk is entirely inside or
             // entirely outside the fiber.
@@ -249,13 +252,13 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             // An update reads a pass's fibers when it needs them (they stay in
             // the stage until this warp's arrival); the sums read them all.
             T sv[CPW][MCH][VEC];
-            T xv[CPW];
-#pragma unroll
-            for (int c = 0; c < CPW; ++c) {
+            auto x_of = [&](const int c) {
                 const int jl = (cg * CPW + c) * FPW + g;
-                if (!UPDATE) load_pass(c, sv[c]);
-                xv[c] = (UPDATE && jl < cw) ? sX[jl] : T(0);
-            }
+                return jl < cw ? sX[jl] : T(0);
+            };
+            if (!UPDATE)
+#pragma unroll
+                for (int c = 0; c < CPW; ++c) load_pass(c, sv[c]);
             if (UPDATE) {
                 const T teps = T(L.eps);
                 // A fiber with X == 0 updates to zero whatever its digamma values
@@ -265,7 +268,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                 unsigned work = 0;
 #pragma unroll
                 for (int c = 0; c < CPW; ++c)
-                    if (__any_sync(0xffffffffu, xv[c] != T(0))) work |= 1u << c;
+                    if (__any_sync(0xffffffffu, x_of(c) != T(0))) work |= 1u << c;
 
                 // The update of one pass from its fiber values se, psi(beta_eph)
                 // values be and X value xe.
@@ -287,6 +290,8 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                         for (int e = 0; e < NC; ++e) ps[e0 + e] = out[e];
                     }
                     T gp[MCH][VEC];
+                    T gm[MCH][VEC];
+                    load_gm(gm);
                     T as = T(0), an = T(0), ad = T(0);
 #pragma unroll
                     for (int m = 0; m < MCH; ++m)
@@ -361,10 +366,8 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                 while (work) {
                     const int c = __ffs(work) - 1;
                     work &= work - 1;
-                    T se[MCH][VEC], be[MCH][VEC], xe = T(0);
-#pragma unroll
-                    for (int cc = 0; cc < CPW; ++cc)
-                        if (cc == c) xe = xv[cc];
+                    T se[MCH][VEC], be[MCH][VEC];
+                    const T xe = x_of(c);
                     load_pass(c, se);
                     {
                         // psi(beta_eph) of the pass's fibers through the read-only
