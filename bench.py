@@ -56,16 +56,25 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profile_traffic(name):
-    """DRAM bytes per launch of the sweep from the committed ncu summary, if any."""
+def profile_value(name, key="traffic_bytes_per_launch"):
+    """A per-launch figure of the sweep (`key: value` line) from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":")[1])
     except OSError:
         pass
     return None
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch of the sweep from the committed ncu summary, if any."""
+    return profile_value(name)
+
+
+# Nominal FP64 vector peak of a B200: 148 SMs x 64 DFMA lanes per cycle x 2 flops x 1965 MHz.
+FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
 
 class ClockSampler:
@@ -327,6 +336,14 @@ def run_ours(args):
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "iteration_ms": iter_ms,
                 "iteration_frac": alg_bytes / (iter_ms / 1e3) / 1e9 / peak}
+    # The secondary ceiling: FP64 arithmetic of the same launch (flops counted by ncu on the
+    # committed profile of this workload, 2*DFMA + DADD + DMUL thread instructions).
+    flop = profile_value(f"sweep_update_plain_1024x1024x64_{args.dtype}.md", "fp64_flop_per_launch")
+    fp64 = None
+    if flop and args.dtype == "f64" and (x, y, z) == (1024, 1024, 64):
+        fp64 = {"flop_per_launch": flop, "achieved_tflops": flop / (kern_ms / 1e3) / 1e12,
+                "peak_tflops": FP64_NOMINAL_TFLOPS, "peak_source": "nominal",
+                "frac": flop / (kern_ms / 1e3) / 1e12 / FP64_NOMINAL_TFLOPS}
 
     # The same solve with skip_zero_rows: bitwise the same S; after the first
     # update, rows whose band segment of X is all zero are neither read nor
@@ -414,7 +431,8 @@ def run_ours(args):
                            "l2": "inputs larger than L2 (S is 512 MiB in f64)",
                            "parallelism": "replicas" if world > 1 else "single GPU"},
                 "hbm_gbs_iteration": alg_bytes / (ms_max / 1e3 / iters) / 1e9,
-                "roofline": roofline, "zero_row_skip": zero_row_skip, "cpu_baseline": cpu,
+                "roofline": roofline, "fp64_arith": fp64, "zero_row_skip": zero_row_skip,
+                "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "S-updates/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
                         "call": "bldm_solve (host X in, device-seeded S0, host S out)"},
