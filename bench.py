@@ -677,6 +677,8 @@ def run_serve(args):
                                              "median": float(np.median(errs)) if errs else None,
                                              "n": len(errs)},
             "gpu_busy_frac": sstats["gpu_ms"] / 1e3 / wall,
+            "gpu_busy_frac_lanes": {"small": (sstats["gpu_ms"] - sstats["gpu_ms_large"]) / 1e3 / wall,
+                                    "large": sstats["gpu_ms_large"] / 1e3 / wall},
             "server": sstats, "clocks": clk.summary()}
     print(json.dumps(line))
     return 0

@@ -76,7 +76,8 @@ class bldm_server_config(ctypes.Structure):
     _fields_ = [("dtype", ctypes.c_int), ("psi_mode", ctypes.c_int), ("eps", ctypes.c_double),
                 ("tol", ctypes.c_double), ("max_iter", ctypes.c_size_t),
                 ("iters_per_round", ctypes.c_size_t), ("max_active", ctypes.c_size_t),
-                ("memory_budget", ctypes.c_size_t), ("rows_per_tile", ctypes.c_int)]
+                ("memory_budget", ctypes.c_size_t), ("rows_per_tile", ctypes.c_int),
+                ("large_elements", ctypes.c_size_t)]
 
 
 class bldm_request_stats(ctypes.Structure):
@@ -91,7 +92,8 @@ class bldm_server_stats(ctypes.Structure):
                [(n, ctypes.c_size_t) for n in ("active", "queued", "bytes_in_use", "bytes_peak",
                                               "budget")] + \
                [("gpu_ms", ctypes.c_double), ("host_ms", ctypes.c_double),
-                ("retiring", ctypes.c_size_t)]
+                ("retiring", ctypes.c_size_t), ("gpu_ms_large", ctypes.c_double),
+                ("retire_ms", ctypes.c_double)]
 
 
 _lib = None
@@ -620,9 +622,10 @@ class Server:
     QUEUED, ACTIVE, DONE, FAILED = 0, 1, 2, 3
 
     def __init__(self, dtype=F32, psi_mode=PSI_APPR, eps=1e-50, tol=1e-6, max_iter=500,
-                 iters_per_round=10, max_active=256, memory_budget=0, rows_per_tile=0):
+                 iters_per_round=10, max_active=256, memory_budget=0, rows_per_tile=0,
+                 large_elements=0):
         cfg = bldm_server_config(dtype, psi_mode, eps, tol, max_iter, iters_per_round, max_active,
-                                 memory_budget, rows_per_tile)
+                                 memory_budget, rows_per_tile, large_elements)
         self.dtype = dtype
         self._h = ctypes.c_void_p()
         self._shapes = {}

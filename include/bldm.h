@@ -369,11 +369,13 @@ int bldm_batch_autotune(bldm_batch* batch, size_t probe_iters, int psi_mode, dou
  * iteration) falls below tol or it has run max_iter iterations (rounded up to
  * a whole round).  Newly admitted requests get their axis sums on their own
  * before joining the round; the others carry theirs over from the previous
- * round.  Retirement runs on a second thread and stream, so the rounds go on
+ * round.  Retirement runs on another thread and stream per lane, so the rounds go on
  * meanwhile: it copies S to the host (in the storage type; fetch converts to
  * FP64), computes log_marginal_S on the device (FP64) and frees the request's
- * device memory.  A request's result does not depend on the other requests
- * being served.
+ * device memory.  Requests of at least large_elements S elements are served
+ * in a second lane with its own worker and a lower-priority stream, so that
+ * the rounds of small requests do not wait for the large ones'.  A request's
+ * result does not depend on the other requests being served.
  * ---------------------------------------------------------------------- */
 typedef struct bldm_server bldm_server;
 typedef struct bldm_server_config {
@@ -386,6 +388,9 @@ typedef struct bldm_server_config {
     size_t max_active;       /* concurrent requests on the device */
     size_t memory_budget;    /* device bytes for requests; 0 = 80% of free */
     int rows_per_tile;       /* 0 = 64 */
+    size_t large_elements;   /* requests with x*y*z >= this are served in a second
+                                lane (own worker thread and lower-priority stream);
+                                0 = 2^25, SIZE_MAX = one lane */
 } bldm_server_config;
 typedef struct bldm_request_stats {
     double queue_ms;         /* submit -> admission */
@@ -401,6 +406,10 @@ typedef struct bldm_server_stats {
     double gpu_ms;           /* device time of the rounds (CUDA events) */
     double host_ms;          /* worker time between rounds (admission, tables) */
     size_t retiring;         /* requests finished on the device, results in flight */
+    double gpu_ms_large;     /* the large-request lane's part of gpu_ms (the two
+                                lanes' rounds overlap, so gpu_ms may exceed wall time) */
+    double retire_ms;        /* retirement threads' time (waiting for the round, result
+                                copies, log-marginal) */
 } bldm_server_stats;
 int bldm_server_create(bldm_server** server, const bldm_server_config* config);
 /* Stops the worker; requests still active or queued are dropped. */

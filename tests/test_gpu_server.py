@@ -54,6 +54,34 @@ def test_alone_equals_in_mix(bldm, workloads, target, seed):
     mix.close()
 
 
+def test_two_lanes_match_one_lane(bldm, workloads):
+    """With a small large_elements the mix is split over both lanes (their own
+    workers and streams, running concurrently); every request's result is
+    bitwise the one of a single-lane server, and the large lane ran rounds."""
+    reqs = [_req(workloads, s, 40 + k) for k, s in enumerate(SHAPES)]
+    results = {}
+    for lanes, large in (("one", 2**64 - 1), ("two", 40000)):
+        srv = bldm.Server(dtype=bldm.F32, tol=1e-5, max_iter=200, iters_per_round=10,
+                          large_elements=large)
+        ids = [srv.submit(X, z, _params(bldm, X.shape[0], z), seed=k)
+               for k, (X, z) in enumerate(reqs)]
+        for rid in ids:
+            assert srv.wait(rid)
+        results[lanes] = [srv.fetch(rid) for rid in ids]
+        st = srv.stats()
+        if lanes == "two":
+            assert st["gpu_ms_large"] > 0.0
+        else:
+            assert st["gpu_ms_large"] == 0.0
+        srv.close()
+    for (S1, st1), (S2, st2) in zip(results["one"], results["two"]):
+        assert st1["status"] == 0 and st2["status"] == 0
+        assert st1["iterations"] == st2["iterations"]
+        np.testing.assert_array_equal(S1, S2)
+    # both lanes had requests
+    assert {x * y * z >= 40000 for x, y, z in SHAPES} == {False, True}
+
+
 def test_server_fp64_matches_oracle_and_stops(bldm, workloads, oracle):
     srv = bldm.Server(dtype=bldm.F64, tol=1e-12, max_iter=30, iters_per_round=10)
     X, z = _req(workloads, (50, 60, 8), 3)
