@@ -169,6 +169,7 @@ SIGNATURES = {
                                          ctypes.c_double, _vp, _vp]),
     "bldm_psi_f64": (ctypes.c_int, [_vp, _sz, ctypes.c_int, _vp, _vp]),
     "bldm_psi_f32": (ctypes.c_int, [_vp, _sz, _vp, _vp]),
+    "bldm_psi_f32_mode": (ctypes.c_int, [_vp, _sz, ctypes.c_int, _vp, _vp]),
     "bldm_log_marginal_S": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _sz, _sz, _dp, _dp,
                                            ctypes.c_double, ctypes.c_double, _dp, _vp]),
     "bldm_bld_fact": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _sz, _sz, ctypes.POINTER(bldm_params),
@@ -531,7 +532,10 @@ def psi(d_in, appr=True, stream=None):
         _check(lib().bldm_psi_f64(_ptr(d_in), d_in.numel(), int(appr), _ptr(out),
                                   _stream_ptr(stream)))
     else:
-        _check(lib().bldm_psi_f32(_ptr(d_in), d_in.numel(), _ptr(out), _stream_ptr(stream)))
+        # FP32: appr == 2 selects the fused sweep's form, anything else the
+        # tabulating form
+        _check(lib().bldm_psi_f32_mode(_ptr(d_in), d_in.numel(), 1 if appr == 2 else 0,
+                                       _ptr(out), _stream_ptr(stream)))
     return out
 
 

@@ -133,13 +133,6 @@ __device__ __forceinline__ double rcp_nr(double d) {
     return fma(y, e, y);
 }
 
-// FP32 reciprocal: hardware approximation refined by one Newton-Raphson step.
-__device__ __forceinline__ float rcp_nr_f32(float d) {
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
-    return fmaf(y, fmaf(-d, y, 1.0f), y);
-}
-
 // Natural logarithm by the table-driven method of P. T. P. Tang ("Table-driven
 // implementation of the logarithm function in IEEE floating-point
 // arithmetic", ACM TOMS 16(4), 1990): x = 2^e m, m in [1,2); R_j = 1/c_j with
@@ -177,7 +170,7 @@ __device__ __forceinline__ double log_tab(double x, const double2* tab) {
     return fma(de, kLn2Hi, t.x) + fma(de, kLn2Lo, l1);
 }
 
-// Reciprocal used by the update: Newton-Raphson in FP64, IEEE in FP32.
+// Reciprocal used by the update and the sweep's digamma.
 template <typename T> struct Rcp;
 template <> struct Rcp<double> {
     __device__ __forceinline__ static double of(double d) {
@@ -186,10 +179,17 @@ template <> struct Rcp<double> {
                                                                                  : 1.0 / d;
     }
 };
+// FP32: the hardware approximation refined by one Newton-Raphson step.  Where
+// the step is undefined (d = 0 or a subnormal d, whose seed is inf; d = inf,
+// whose seed is 0) the refinement gives NaN and the seed itself is returned:
+// inf as 1/d overflows, 0 for an infinite divisor.  A reciprocal in the
+// subnormal range (|d| >= 2^126) flushes to 0.
 template <> struct Rcp<float> {
     __device__ __forceinline__ static float of(float d) {
-        const float a = fabsf(d);
-        return (a >= 1.17549435e-38f && a <= 8.5e37f) ? rcp_nr_f32(d) : 1.0f / d;
+        float y;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
+        const float r = fmaf(y, fmaf(-d, y, 1.0f), y);
+        return r == r ? r : y;
     }
 };
 
@@ -254,43 +254,30 @@ template <> struct PsiPass<double, false> {
         for (int e = 0; e < NE; ++e) out[e] = psi_exact_f64(x[e]);
     }
 };
-// FP32 digamma for the sweep: psi_f32's shift rule and series, with a
-// hardware reciprocal refined by one Newton-Raphson step and the hardware
-// base-2 logarithm (relative error about 2^-21, at the resolution of FP32 S).
-
+// FP32 digamma for the sweep.  Arguments below 4 take exactly three steps of
+// the recurrence psi(v) = psi(v + 3) - (1/v + 1/(v+1) + 1/(v+2)), the three
+// reciprocals summed as one rational function (3v^2 + 6v + 2) / (v (v+1) (v+2));
+// at v + 3 >= 4 (and at v >= 4 unshifted) the asymptotic series
+// ln x - 1/(2x) - sum_k B_2k / (2k x^2k), truncated after the x^-10 term,
+// leaves a remainder below 1.3e-9, under FP32 resolution.  One reciprocal of
+// x q serves both 1/x and the shift's division; the logarithm is the hardware
+// base-2 one (relative error about 2^-21, at the resolution of FP32 S).  No
+// per-step selects: the shift is a fixed polynomial evaluation.
 template <int NE>
 __device__ __forceinline__ void psi_f32_batch(const float (&x)[NE], float (&out)[NE]) {
-    int n[NE];
-    float num[NE], den[NE];
-    bool six = false;
 #pragma unroll
     for (int e = 0; e < NE; ++e) {
-        n[e] = (x[e] < 1.0f) ? 6 : ((x[e] < 6.0f) ? 6 - __float2int_rz(x[e]) : 0);
-        six |= n[e] == 6;
-        num[e] = 0.0f;
-        den[e] = 1.0f;
-    }
-    const int steps = __any_sync(0xffffffffu, six) ? 6 : 5;
-#pragma unroll
-    for (int m = 0; m < 6; ++m) {
-        if (m == 5 && steps == 5) break;
-#pragma unroll
-        for (int e = 0; e < NE; ++e) {
-            const bool act = m < n[e];
-            const float f = act ? x[e] + float(m) : 1.0f;
-            num[e] = act ? fmaf(num[e], f, den[e]) : num[e];
-            den[e] *= f;
-        }
-    }
-#pragma unroll
-    for (int e = 0; e < NE; ++e) {
-        const float xs = x[e] + float(n[e]);
-        const float pd = xs * den[e];
-        const float inv = (pd >= 1.17549435e-38f && pd <= 8.5e37f) ? rcp_nr_f32(pd) : 1.0f / pd;
-        const float r = den[e] * inv;
-        const float shift = num[e] * xs * inv;
+        const float v = x[e];
+        const bool lo = v < 4.0f;
+        const float q = lo ? fmaf(v + 3.0f, v, 2.0f) * v : 1.0f;   // v (v+1) (v+2)
+        const float p = lo ? fmaf(fmaf(3.0f, v, 6.0f), v, 2.0f) : 0.0f;
+        const float xs = lo ? v + 3.0f : v;
+        const float inv = Rcp<float>::of(xs * q);
+        const float r = q * inv;              // 1 / xs
+        const float shift = (p * xs) * inv;   // p / q
         const float r2 = r * r;
-        float t = fmaf(r2, -1.f / 240.f, 1.f / 252.f);
+        float t = fmaf(r2, -1.f / 132.f, 1.f / 240.f);
+        t = fmaf(r2, -t, 1.f / 252.f);
         t = fmaf(r2, -t, 1.f / 120.f);
         t = fmaf(r2, -t, 1.f / 12.f);
         out[e] = __logf(xs) - 0.5f * r - r2 * t - shift;

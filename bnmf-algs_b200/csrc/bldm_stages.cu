@@ -126,9 +126,17 @@ __global__ void psi_f64_kernel(const double* in, long long n, int appr, double* 
     }
     if (e < n) out[e] = appr ? psi_appr_f64(in[e]) : psi_exact_f64(in[e]);
 }
-__global__ void psi_f32_kernel(const float* in, long long n, float* out) {
+__global__ void psi_f32_kernel(const float* in, long long n, int mode, float* out) {
     const long long e = (long long)blockIdx.x * kT + threadIdx.x;
-    if (e < n) out[e] = psi_f32(in[e]);
+    if (e >= n) return;
+    if (mode == 1) {
+        const float a[1] = {in[e]};
+        float o[1];
+        psi_f32_batch<1>(a, o);
+        out[e] = o[0];
+    } else {
+        out[e] = psi_f32(in[e]);
+    }
 }
 
 // ---- log_marginal_S (src/alloc_model/alloc_model_funcs.hpp:33-194,573-586).
@@ -317,13 +325,18 @@ int bldm_psi_f64(const double* d_in, size_t n, int appr, double* d_out, void* st
     return cuda_status(cudaGetLastError());
 }
 
-int bldm_psi_f32(const float* d_in, size_t n, float* d_out, void* stream) {
+int bldm_psi_f32_mode(const float* d_in, size_t n, int mode, float* d_out, void* stream) {
     BLDM_CHECK_PTR(d_in);
     BLDM_CHECK_PTR(d_out);
+    if (mode != 0 && mode != 1) return BLDM_ERR_BAD_ARG;
     if (n == 0) return BLDM_OK;
     psi_f32_kernel<<<nblocks((long long)n), kT, 0, static_cast<cudaStream_t>(stream)>>>(
-        d_in, (long long)n, d_out);
+        d_in, (long long)n, mode, d_out);
     return cuda_status(cudaGetLastError());
+}
+
+int bldm_psi_f32(const float* d_in, size_t n, float* d_out, void* stream) {
+    return bldm_psi_f32_mode(d_in, n, 0, d_out, stream);
 }
 
 int bldm_log_marginal_S(const void* d_S, int dtype, size_t x, size_t y, size_t z,

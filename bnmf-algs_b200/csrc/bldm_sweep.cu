@@ -315,10 +315,17 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
     int cps = (tune && tune->ctas_per_sm > 0) ? tune->ctas_per_sm : 2;
     if (cps > 2) return BLDM_ERR_UNSUPPORTED;
     const size_t budget = (cps == 2 ? 110 : 220) * 1024;
-    long st = budget > fixed ? long((budget - fixed) / per_stage) : 0;
-    st = std::min(8L, st);
+    long st_max = budget > fixed ? long((budget - fixed) / per_stage) : 0;
+    st_max = std::min(8L, st_max);
+    // Default ring depth: about kRingBytes of copies per CTA (two CTAs per SM)
+    // cover the memory latency; deeper rings add DRAM contention without
+    // hiding more (1024x1024x64 update: 4 stages of 17 KB beat 5 in FP64 and
+    // FP32, and all-zero X streams fastest at 2-3).
+    constexpr long kRingBytes = 64 * 1024;
+    long st = std::min(st_max, std::max(2L, long((kRingBytes + c.stage_bytes - 1) / c.stage_bytes)));
+    if (st_max < 2) st = st_max;
     if (tune && tune->stages > 0) {
-        if (tune->stages > st || tune->stages < 2) return BLDM_ERR_UNSUPPORTED;
+        if (tune->stages > st_max || tune->stages < 2) return BLDM_ERR_UNSUPPORTED;
         st = tune->stages;
     }
     if (st < 2) {
@@ -328,8 +335,11 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
         st = std::min(8L, long((220 * 1024 - fixed) / per_stage));
         if (st < 2) return BLDM_ERR_UNSUPPORTED;
     }
-    c.stages = int(st);
     // the end-of-tile S_pjk combine reuses the drained ring: [rows/stage][band_w][z]
+    const size_t combine = size_t(kSweepWarps / c.wpr) * c.band_w * z * 8;
+    if (!(tune && tune->stages > 0))
+        while (c.wpr < kSweepWarps && combine > size_t(st) * c.stage_bytes && st < st_max) ++st;
+    c.stages = int(st);
     if (c.wpr < kSweepWarps &&
         size_t(kSweepWarps / c.wpr) * c.band_w * z * 8 > size_t(c.stages) * c.stage_bytes)
         return BLDM_ERR_UNSUPPORTED;

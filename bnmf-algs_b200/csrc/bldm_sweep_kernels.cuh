@@ -16,6 +16,11 @@ template <typename T, int VEC> struct VecIO {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) __stcs(p + e, v[e]);
     }
+    // through the read-only data cache
+    __device__ __forceinline__ static void ldg(const T* p, T (&v)[VEC]) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) v[e] = __ldg(p + e);
+    }
 };
 template <> struct VecIO<double, 2> {
     __device__ __forceinline__ static void load(const double* p, double (&v)[2]) {
@@ -25,6 +30,11 @@ template <> struct VecIO<double, 2> {
     }
     __device__ __forceinline__ static void store(double* p, const double (&v)[2]) {
         __stcs(reinterpret_cast<double2*>(p), make_double2(v[0], v[1]));
+    }
+    __device__ __forceinline__ static void ldg(const double* p, double (&v)[2]) {
+        const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+        v[0] = t.x;
+        v[1] = t.y;
     }
 };
 template <> struct VecIO<float, 4> {
@@ -37,6 +47,13 @@ template <> struct VecIO<float, 4> {
     }
     __device__ __forceinline__ static void store(float* p, const float (&v)[4]) {
         __stcs(reinterpret_cast<float4*>(p), make_float4(v[0], v[1], v[2], v[3]));
+    }
+    __device__ __forceinline__ static void ldg(const float* p, float (&v)[4]) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
     }
 };
 
@@ -129,8 +146,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
     // Round t holds entries t*RPS + r, r < RPS, of the row sequence; a compact
     // update records their rows in srow[stage] for the consumers (published
     // by the stage's mbarrier arrival, read after its wait).
-    auto issue = [&](int t) {
-        const int s = t % L.stages;
+    auto issue = [&](int t, int s) {
         unsigned char* st = stage0 + (size_t)s * L.stage_bytes;
         const int nr = min(RPS, nlist - t * RPS);
         uint32_t tot = 0;
@@ -171,7 +187,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
 
     if (tid == 0) {
         const int n0 = min(L.stages, nrounds);
-        for (int t = 0; t < n0; ++t) issue(t);
+        for (int t = 0; t < n0; ++t) issue(t, t);
     }
 
     // S_pjk accumulators of the lane's fibers over the tile's rows.
@@ -186,11 +202,12 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
     const bool track = BATCH && UPDATE && in.delta_part != nullptr;
     double d_abs = 0.0, d_new = 0.0;
 
+    // round t uses stage s = t % stages in its lap-th pass over the ring
+    // (counted, not divided: the ring depth is a launch parameter)
+    int s = 0, lap = 0;
     for (int t = 0; t < nrounds; ++t) {
-        const int s = t % L.stages;
         // warp-uniform: the lane-group shuffles below need every lane of the warp
-        const bool ok =
-            __all_sync(0xffffffffu, mbar_wait_bounded(&bars[s], (uint32_t)((t / L.stages) & 1)));
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&bars[s], (uint32_t)(lap & 1)));
         if (!ok) {
             // Give up: flag the error and wait (bounded) for the copies that
             // may still be landing in this CTA's shared memory.
@@ -212,6 +229,8 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         for (int m = 0; m < MCH; ++m)
 #pragma unroll
             for (int v = 0; v < VEC; ++v) ip[m][v].init();
+        // warp-uniform: an update round without a pass with X != 0 leaves ip at zero
+        bool ip_live = !UPDATE;
 
         if (row_ok) {
             const uintptr_t aS = reinterpret_cast<uintptr_t>(in.S + (i * in.y + c0) * z);
@@ -269,6 +288,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
 #pragma unroll
                 for (int c = 0; c < CPW; ++c)
                     if (__any_sync(0xffffffffu, x_of(c) != T(0))) work |= 1u << c;
+                ip_live = work != 0;
 
                 // The update of one pass from its fiber values se, psi(beta_eph)
                 // values be and X value xe.
@@ -375,13 +395,15 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                         // out of registers, which the digamma arithmetic needs more
                         const int jl = (cg * CPW + c) * FPW + g;
 #pragma unroll
-                        for (int m = 0; m < MCH; ++m)
+                        for (int m = 0; m < MCH; ++m) {
+                            const long long k0 = (long long)(m * LPF + q) * VEC;
+                            if (jl < cw && k0 < z) {
+                                VecIO<T, VEC>::ldg(in.psiB + (c0 + jl) * z + k0, be[m]);
+                            } else {
 #pragma unroll
-                            for (int v = 0; v < VEC; ++v) {
-                                const long long k = (long long)(m * LPF + q) * VEC + v;
-                                be[m][v] = (jl < cw && k < z) ? __ldg(in.psiB + (c0 + jl) * z + k)
-                                                              : T(0);
+                                for (int v = 0; v < VEC; ++v) be[m][v] = T(0);
                             }
+                        }
                     }
                     T sn[MCH][VEC];
                     pass_math(se, be, xe, sn);
@@ -410,13 +432,17 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         }
 
         // S_ipk partial of row i over this warp's columns -> red[s][warp].
+        // (zeros stored directly when ip is zero: no conversion, no shuffles)
         double* redw = red + ((size_t)s * NW + warp) * z;
 #pragma unroll
         for (int m = 0; m < MCH; ++m)
 #pragma unroll
             for (int v = 0; v < VEC; ++v) {
-                double val = ip[m][v].value();
-                if (FPW > 1) val = cross_group_sum<LPF>(val);
+                double val = 0.0;
+                if (ip_live) {
+                    val = ip[m][v].value();
+                    if (FPW > 1) val = cross_group_sum<LPF>(val);
+                }
                 const long long k = (long long)(m * LPF + q) * VEC + v;
                 if (g == 0 && k < z) redw[k] = val;
             }
@@ -429,7 +455,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         int last = 0;
         if (lane == 0) {
             __threadfence_block();
-            last = (atomicAdd(&cnt[s], 1) == (t / L.stages + 1) * NW - 1) ? 1 : 0;
+            last = (atomicAdd(&cnt[s], 1) == (lap + 1) * NW - 1) ? 1 : 0;
         }
         last = __shfl_sync(0xffffffffu, last, 0);
         if (last) {
@@ -451,7 +477,11 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                 }
             }
             __syncwarp();
-            if (lane == 0 && t + L.stages < nrounds) issue(t + L.stages);
+            if (lane == 0 && t + L.stages < nrounds) issue(t + L.stages, s);
+        }
+        if (++s == L.stages) {
+            s = 0;
+            ++lap;
         }
     }
 

@@ -255,7 +255,13 @@ int bldm_update_S_f64(const double* d_X, const double* d_nom,
  * 2 psi_appr as evaluated inside the fused sweep (same function, batched
  * form with Newton-Raphson reciprocals and a table logarithm). */
 int bldm_psi_f64(const double* d_in, size_t n, int appr, double* d_out, void* stream);
+/* FP32 digamma for FP32 storage: mode 0 the form that tabulates psi(alpha_eph)
+ * and psi(beta_eph) (IEEE division, libm logarithm), mode 1 the form the
+ * fused FP32 sweep evaluates for psi(S+1) (three-step rational shift,
+ * Newton-Raphson reciprocal, hardware logarithm).  The reference evaluates
+ * util::psi_appr (src/util/util.hpp:440-514) in the storage type. */
 int bldm_psi_f32(const float* d_in, size_t n, float* d_out, void* stream);
+int bldm_psi_f32_mode(const float* d_in, size_t n, int mode, float* d_out, void* stream);
 
 /* alloc_model::log_marginal_S (src/alloc_model/alloc_model_funcs.hpp:573-586)
  * of a device tensor, computed on the device in FP64.  d_S is FP64 or FP32

@@ -46,11 +46,15 @@ def test_psi_appr_and_exact_match_oracle(bldm, oracle, psi_points):
         assert err.max() <= 2e-14, (mode, err.max(), pts[err.argmax()])
 
 
-def test_psi_f32(bldm):
+@pytest.mark.parametrize("mode", [1, 2])   # 1: tabulating form, 2: the FP32 sweep's form
+def test_psi_f32(bldm, mode):
     from scipy.special import digamma
     rng = np.random.default_rng(1)
-    pts = np.concatenate([rng.uniform(1, 7, 4000), rng.lognormal(2, 3, 4000)]).astype(np.float32)
-    got = host(bldm.psi(dev(pts, torch.float32))).astype(np.float64)
+    # the sweep evaluates psi(S + 1) >= 1; both forms also cover (0, 1) and
+    # counts up to ~1e8 through the lognormal draws
+    pts = np.concatenate([rng.uniform(1, 7, 4000), rng.uniform(3.9, 4.1, 2000),
+                          rng.lognormal(2, 3, 4000), [1.0, 3.0, 4.0, 1e8]]).astype(np.float32)
+    got = host(bldm.psi(dev(pts, torch.float32), appr=mode)).astype(np.float64)
     ref = digamma(pts.astype(np.float64))
     assert (np.abs(got - ref) / np.maximum(1.0, np.abs(ref))).max() <= 2e-6
 
