@@ -31,25 +31,23 @@
 namespace bldm {
 
 // Sum of p[r * stride], r < n, in increasing r (the order of a plain loop),
-// with the loads of eight terms issued before their adds so that a thread keeps
-// eight reads of the partial buffers in flight.
+// with the loads of sixteen terms issued before their adds so that a thread
+// keeps sixteen reads of the partial buffers in flight (the partials were just
+// written, so the finalize waits on L2 round trips, not on bandwidth).  Terms
+// past n load nothing and add an exact 0.0.
 template <bool CG>
 __device__ __forceinline__ double sum_strided(const double* p, long long stride, int n) {
+    constexpr int W = 16;
     double s = 0.0;
-    int r = 0;
-    for (; r + 8 <= n; r += 8) {
-        double v[8];
+    for (int r = 0; r < n; r += W) {
+        double v[W];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < W; ++u) {
             const double* a = p + (long long)(r + u) * stride;
-            v[u] = CG ? __ldcg(a) : *a;
+            v[u] = (r + u < n) ? (CG ? __ldcg(a) : *a) : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) s += v[u];
-    }
-    for (; r < n; ++r) {
-        const double* a = p + (long long)r * stride;
-        s += CG ? __ldcg(a) : *a;
+        for (int u = 0; u < W; ++u) s += v[u];
     }
     return s;
 }
@@ -355,10 +353,12 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
     c.n_rr = int(nrr);
     c.rr_base = int(x / nrr);
     c.rr_extra = int(x % nrr);
-    // finalize row blocks
+    // finalize row blocks: one row per thread (R rows of KT columns per block)
+    // up to ~256 blocks, so that a thread's sums of the band partials are not
+    // serialised over several rows
     const int KT = int(std::min<size_t>(z, kFinThreads));
     const int R = kFinThreads / KT;
-    long rows = std::max<long>(R, long((x + 127) / 128));
+    long rows = std::max<long>(R, long((x + 255) / 256));
     c.rows_per_ablk = int(rows);
     c.n_ablk = int((x + rows - 1) / rows);
     c.fin_threads = kFinThreads;
