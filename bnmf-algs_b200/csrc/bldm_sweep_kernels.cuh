@@ -224,11 +224,14 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         const long long i =
             compact ? (row_ok ? (long long)srow[s][rs] : 0) : r0 + (long long)t * RPS + rs;
 
-        Acc<T> ip[MCH][VEC];
+        // S_ipk of row i over this warp's passes: at most CPW terms per lane,
+        // accumulated in FP64 (exact for so few storage-type terms, and cheaper
+        // than a Kahan pair in FP32)
+        double ip[MCH][VEC];
 #pragma unroll
         for (int m = 0; m < MCH; ++m)
 #pragma unroll
-            for (int v = 0; v < VEC; ++v) ip[m][v].init();
+            for (int v = 0; v < VEC; ++v) ip[m][v] = 0.0;
         // warp-uniform: an update round without a pass with X != 0 leaves ip at zero
         bool ip_live = !UPDATE;
 
@@ -349,7 +352,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                     for (int m = 0; m < MCH; ++m) {
 #pragma unroll
                         for (int v = 0; v < VEC; ++v) {
-                            ip[m][v].add(sn[m][v]);
+                            ip[m][v] += double(sn[m][v]);
                             if (track) {
                                 d_abs += fabs(double(sn[m][v]) - double(se[m][v]));
                                 d_new += fabs(double(sn[m][v]));
@@ -426,7 +429,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
 #pragma unroll
                         for (int v = 0; v < VEC; ++v) {
                             pj[c][m][v].add(sv[c][m][v]);
-                            ip[m][v].add(sv[c][m][v]);
+                            ip[m][v] += double(sv[c][m][v]);
                         }
             }
         }
@@ -440,7 +443,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             for (int v = 0; v < VEC; ++v) {
                 double val = 0.0;
                 if (ip_live) {
-                    val = ip[m][v].value();
+                    val = ip[m][v];
                     if (FPW > 1) val = cross_group_sum<LPF>(val);
                 }
                 const long long k = (long long)(m * LPF + q) * VEC + v;
