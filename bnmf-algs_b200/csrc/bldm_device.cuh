@@ -93,7 +93,7 @@ __device__ __forceinline__ float psi_f32(float x) {
     const float xs = x + n;
     const float inv = 1.f / (xs * den);
     const float r = den * inv;
-    const float shift = num * xs * inv;
+    const float shift = n > 0.f ? num * xs * inv : 0.f;  // no 0 * inf at x = inf
     const float r2 = r * r;
     float t = fmaf(r2, -1.f / 240.f, 1.f / 252.f);
     t = fmaf(r2, -t, 1.f / 120.f);
@@ -274,7 +274,7 @@ __device__ __forceinline__ void psi_f32_batch(const float (&x)[NE], float (&out)
         const float xs = lo ? v + 3.0f : v;
         const float inv = Rcp<float>::of(xs * q);
         const float r = q * inv;              // 1 / xs
-        const float shift = (p * xs) * inv;   // p / q
+        const float shift = lo ? (p * xs) * inv : 0.0f;   // p / q (no 0 * inf at v = inf)
         const float r2 = r * r;
         float t = fmaf(r2, -1.f / 132.f, 1.f / 240.f);
         t = fmaf(r2, -t, 1.f / 252.f);

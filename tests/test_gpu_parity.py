@@ -57,6 +57,9 @@ def test_psi_f32(bldm, mode):
     got = host(bldm.psi(dev(pts, torch.float32), appr=mode)).astype(np.float64)
     ref = digamma(pts.astype(np.float64))
     assert (np.abs(got - ref) / np.maximum(1.0, np.abs(ref))).max() <= 2e-6
+    # psi(+inf) = +inf
+    inf = host(bldm.psi(dev(np.array([np.inf], np.float32), torch.float32), appr=mode))
+    assert np.isposinf(inf[0]), inf
 
 
 # ------------------------------------------------- per-stage (reference funcs tests)
