@@ -31,13 +31,14 @@
 namespace bldm {
 
 // Sum of p[r * stride], r < n, in increasing r (the order of a plain loop),
-// with the loads of sixteen terms issued before their adds so that a thread
-// keeps sixteen reads of the partial buffers in flight (the partials were just
-// written, so the finalize waits on L2 round trips, not on bandwidth).  Terms
-// past n load nothing and add an exact 0.0.
-template <bool CG>
+// with the loads of W terms issued before their adds so that a thread keeps W
+// reads of the partial buffers in flight (the partials were just written, so
+// the finalize waits on L2 round trips, not on bandwidth).  Terms past n load
+// nothing and add an exact 0.0.  W = 16 for the single-instance finalize (few
+// blocks, long sums); 8 for the multi-instance one, whose tens of thousands of
+// short blocks need the occupancy that fewer registers give.
+template <bool CG, int W>
 __device__ __forceinline__ double sum_strided(const double* p, long long stride, int n) {
-    constexpr int W = 16;
     double s = 0.0;
     for (int r = 0; r < n; r += W) {
         double v[W];
@@ -58,7 +59,7 @@ __device__ __forceinline__ double sum_strided(const double* p, long long stride,
 // the block sums (R interleaved groups of blocks, then the groups in order),
 // tabulates psi(sum_i alpha_eph(i,k)) and, when the sweep tracked it, the
 // relative change of S.
-template <typename T>
+template <typename T, int W>
 __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int plus_appr,
                                                int minus_appr) {
     const long long z = p.z;
@@ -67,7 +68,7 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
         const long long idx = (long long)blk * kFinThreads + tid;
         if (idx < p.y * z) {
             const long long k = idx % z;
-            const double s = sum_strided<false>(p.part_pjk + idx, p.y * z, p.n_rr);
+            const double s = sum_strided<false, W>(p.part_pjk + idx, p.y * z, p.n_rr);
             if (p.red)
                 p.red[idx] = s;
             else
@@ -87,7 +88,7 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
         for (long long k = tid % KT; k < z; k += KT) {
             double a = 0.0;
             for (long long i = i0 + sub; i < i1; i += R) {
-                const double s = sum_strided<false>(p.part_ipk + i * z + k, p.x * z, p.n_bands);
+                const double s = sum_strided<false, W>(p.part_ipk + i * z + k, p.x * z, p.n_bands);
                 const double ae = s + p.alpha[i];
                 p.psiA[i * z + k] = T(psi_mode_f64(ae, minus_appr != 0));
                 a += ae;
@@ -112,7 +113,7 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
             for (long long k = tid % KT; k < z; k += KT) {
                 const int nb = (p.n_ablk - sub + R - 1) / R;
                 acc[sub * z + k] =
-                    sum_strided<true>(p.asum_part + (long long)sub * z + k, (long long)R * z, nb);
+                    sum_strided<true, W>(p.asum_part + (long long)sub * z + k, (long long)R * z, nb);
             }
         }
         __syncthreads();
@@ -146,7 +147,7 @@ template <typename T>
 __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const FinParams<T> p) {
     grid_dep_wait();  // the sweep's partials
     grid_dep_launch();
-    finalize_block<T>(p.f, int(blockIdx.x), p.plus_appr, p.minus_appr);
+    finalize_block<T, 16>(p.f, int(blockIdx.x), p.plus_appr, p.minus_appr);
 }
 
 // Row-sharded solves: the digamma tables of the shared sums once every shard's
@@ -160,8 +161,10 @@ __global__ void __launch_bounds__(kFinThreads)
     if (idx < z) psiAS[idx] = T(psi_mode_f64(red[y * z + idx], minus_appr != 0));
 }
 
+// Five resident blocks per SM (48 registers, no spills): a batch's finalize is
+// tens of thousands of short, latency-bound blocks, so occupancy sets its pace.
 template <typename T>
-__global__ void __launch_bounds__(kFinThreads) finalize_batch_kernel(const BatchFinParams<T> p) {
+__global__ void __launch_bounds__(kFinThreads, 5) finalize_batch_kernel(const BatchFinParams<T> p) {
     // instance owning this block: last i with block_off[i] <= blockIdx.x
     int lo = 0, hi = p.n_inst - 1;
     const int b = int(blockIdx.x);
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(kFinThreads) finalize_batch_kernel(const Batch
         else hi = mid - 1;
     }
     const FinInst<T> f = p.insts[lo];
-    finalize_block<T>(f, b - p.block_off[lo], p.plus_appr, p.minus_appr);
+    finalize_block<T, 8>(f, b - p.block_off[lo], p.plus_appr, p.minus_appr);
 }
 
 void* finalize_batch_fn(int dtype) {
