@@ -196,15 +196,41 @@ __device__ __forceinline__ double exp1_variate(uint64_t hseed, uint64_t fiber, u
     return -log(u);
 }
 
+// Lane groups of lpf = min(32, pow2ceil(z)) lanes per fiber, 32 / lpf fibers
+// per warp: lane q draws k = q, q + lpf, ...; the first four draws per lane stay
+// in registers (each variate computed once for z <= 4 lpf; beyond that the rest
+// are drawn again for the stores); the group adds the fiber's total by
+// shuffles and the stores of consecutive lanes are consecutive elements.
 template <typename T>
-__global__ void init_S_kernel(const T* X, T* S, long long nf, long long z, uint64_t seed) {
-    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= nf) return;
+__global__ void init_S_kernel(const T* X, T* S, long long nf, long long z, uint64_t seed,
+                              int lpf) {
+    constexpr int R = 4;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long f = gw * (32 / lpf) + lane / lpf;
+    const int q = lane % lpf;
+    const bool on = f < nf;
     const uint64_t hs = splitmix64(seed ^ 0x5DEECE66Dull);
+    double v[R];
     double tot = 0.0;
-    for (long long k = 0; k < z; ++k) tot += exp1_variate(hs, (uint64_t)f, (uint64_t)k);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const long long k = q + (long long)r * lpf;
+        v[r] = (on && k < z) ? exp1_variate(hs, (uint64_t)f, (uint64_t)k) : 0.0;
+        tot += v[r];
+    }
+    for (long long k = q + (long long)R * lpf; k < z; k += lpf)
+        tot += on ? exp1_variate(hs, (uint64_t)f, (uint64_t)k) : 0.0;
+    // every lane takes part in the shuffles; groups are lpf-aligned
+    for (int o = 1; o < lpf; o <<= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (!on) return;
     const double xv = double(X[f]);
-    for (long long k = 0; k < z; ++k)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const long long k = q + (long long)r * lpf;
+        if (k < z) S[f * z + k] = T(xv * (v[r] / tot));
+    }
+    for (long long k = q + (long long)R * lpf; k < z; k += lpf)
         S[f * z + k] = T(xv * (exp1_variate(hs, (uint64_t)f, (uint64_t)k) / tot));
 }
 
@@ -713,18 +739,10 @@ int plan_run(PlanImpl* p, const void* dX, const double* dalpha, const double* db
 }
 
 int plan_init_S(PlanImpl* p, const void* dX, void* dS, uint64_t seed, cudaStream_t st) {
-    const long long nf = (long long)(p->x * p->y);
-    const unsigned blocks = unsigned((nf + 255) / 256);
-    if (p->dtype == BLDM_F64)
-        init_S_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(dX),
-                                                      static_cast<double*>(dS), nf,
-                                                      (long long)p->z, seed);
-    else
-        init_S_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const float*>(dX),
-                                                     static_cast<float*>(dS), nf,
-                                                     (long long)p->z, seed);
+    const int rc = launch_init_S(p->dtype, dX, dS, (long long)(p->x * p->y), (long long)p->z,
+                                 seed, st);
     p->launches += 1;
-    return cuda_status(cudaGetLastError());
+    return rc;
 }
 
 // One warp per (row, band): nz_rows[b][i] = 1 when row i has a nonzero X in
@@ -786,13 +804,17 @@ int launch_nz_rows(int dtype, const void* dX, long long x, long long y, int band
 
 int launch_init_S(int dtype, const void* dX, void* dS, long long nf, long long z, uint64_t seed,
                   cudaStream_t st) {
-    const unsigned blocks = unsigned((nf + 255) / 256);
+    if (nf <= 0 || z <= 0) return BLDM_OK;
+    int lpf = 1;
+    while (lpf < 32 && lpf < z) lpf <<= 1;
+    const long long warps = (nf + (32 / lpf) - 1) / (32 / lpf);
+    const unsigned blocks = unsigned((warps * 32 + 255) / 256);
     if (dtype == BLDM_F64)
         init_S_kernel<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(dX),
-                                                      static_cast<double*>(dS), nf, z, seed);
+                                                      static_cast<double*>(dS), nf, z, seed, lpf);
     else
         init_S_kernel<float><<<blocks, 256, 0, st>>>(static_cast<const float*>(dX),
-                                                     static_cast<float*>(dS), nf, z, seed);
+                                                     static_cast<float*>(dS), nf, z, seed, lpf);
     return cuda_status(cudaGetLastError());
 }
 

@@ -229,13 +229,17 @@ def test_solver_is_deterministic(bldm, workloads):
 def test_device_init_S_matches_oracle(bldm, oracle):
     rng = np.random.default_rng(10)
     X = rng.poisson(5.0, (50, 70)).astype(float)
-    plan = bldm.Plan(50, 70, 9)
-    dX = dev(X)
-    dS = torch.empty((50, 70, 9), dtype=torch.float64, device="cuda")
-    plan.init_S(dX, dS, seed=77)
-    got = host(dS)
-    ref = oracle.init_S(X, 9, 77)
-    assert rel_err(got, ref) <= 1e-14
+    # lane groups narrower than a warp (z = 1, 9), four draws per lane kept in
+    # registers (z = 64) and draws beyond them made again for the stores (z = 200)
+    for zz in (1, 64, 200, 9):
+        plan = bldm.Plan(50, 70, zz)
+        dS = torch.empty((50, 70, zz), dtype=torch.float64, device="cuda")
+        plan.init_S(dev(X), dS, seed=77)
+        got = host(dS)
+        ref = oracle.init_S(X, zz, 77)
+        assert rel_err(got, ref) <= 1e-14, zz
+        if zz != 9:
+            plan.close()
     # a solve with S0=None starts from the same tensor
     params = bldm.Params(1, 1, np.ones(50), np.ones(9))
     S1 = bldm.bld_mult(X, 9, params, 3, True, seed=77)
