@@ -831,7 +831,8 @@ def main():
                     help="serving loop: Poisson arrivals at --rate req/s for --duration s; "
                          "p50/p99 latency, solves/s, log-marginal error vs FP64")
     ap.add_argument("--rate", type=float, default=50.0)
-    ap.add_argument("--duration", type=float, default=20.0)
+    ap.add_argument("--duration", type=float, default=60.0,
+                    help="seconds of Poisson traffic for --serve (the serving workload runs 60 s)")
     ap.add_argument("--fp64-sample", type=int, default=16)
     ap.add_argument("--precision", action="store_true",
                     help="precision study: 2048x2048x32 heavy-tailed X, FP32 (compensated sums) "
