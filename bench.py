@@ -57,20 +57,46 @@ def hbm_peak():
 
 
 def profile_value(name, key="traffic_bytes_per_launch"):
-    """A per-launch figure of the sweep (`key: value` line) from the committed ncu summary."""
+    """A per-launch figure of the sweep (`key: value` line) from a committed ncu
+    summary under profiles/, with where it came from: these figures are read
+    from the capture, not measured by this run."""
     path = os.path.join(ROOT, "profiles", name)
+    val, kernel_build = None, None
     try:
         for line in open(path):
             if line.startswith(key + ":"):
-                return float(line.split(":")[1])
+                val = float(line.split(":")[1])
+            if line.startswith("kernel_source_sha:"):
+                kernel_build = line.split(":", 1)[1].strip()
     except OSError:
         pass
-    return None
+    if val is None:
+        return None, None
+    src = f"profiles/{name} (ncu capture"
+    src += f" of kernel sources {kernel_build})" if kernel_build else ")"
+    return val, src
 
 
-def profile_traffic(name):
-    """DRAM bytes per launch of the sweep from the committed ncu summary, if any."""
-    return profile_value(name)
+def kernel_source_sha():
+    """Digest of the sweep kernel sources, to compare with a profile's
+    kernel_source_sha line: equal means the capture is of this build's kernel."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in ("bldm_sweep_kernels.cuh", "bldm_device.cuh", "bldm_kernels.h"):
+        with open(os.path.join(PKG_DIR, "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:12]
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
 
 
 # Nominal FP64 vector peak of a B200: 148 SMs x 64 DFMA lanes per cycle x 2 flops x 1965 MHz.
@@ -133,9 +159,10 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def cpu_baseline_oracle(prob, target_s=10.0, threads=0):
+def cpu_baseline_oracle(prob, target_s=10.0, threads=0, small=None):
     """The oracle (reference restatement, OpenMP) on a bounded sample: whole
-    iterations of the same workload, as many as fit in about target_s."""
+    iterations of the same workload, as many as fit in about target_s; with
+    `small`, also the CPU-runnable 64x48x8 workload's whole 200-iteration solve."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     cores = O.set_threads(threads)
@@ -149,9 +176,23 @@ def cpu_baseline_oracle(prob, target_s=10.0, threads=0):
     O.bld_mult(X, z, prob["alpha"], prob["beta"], n, O.PSI_APPR, 1e-50, S0=S0)
     dt = time.perf_counter() - t0
     upd = X.size * z * n
-    return {"value": upd / dt, "unit": "S-updates/s", "cores": cores, "kind": "port",
-            "sample": f"{n} iterations of the full {X.shape[0]}x{X.shape[1]}x{z} workload "
-                      f"({dt:.1f} s, FP64, psi_appr, OpenMP {cores} threads)"}
+    out = {"value": upd / dt, "unit": "S-updates/s", "cores": cores, "kind": "port",
+           "cpu_model": cpu_model(), "nproc": os.cpu_count(),
+           "sample": f"{n} iterations of the full {X.shape[0]}x{X.shape[1]}x{z} workload "
+                     f"({dt:.1f} s, FP64, psi_appr, OpenMP {cores} threads)"}
+    if small is not None:
+        Xs, zs, it = small["X"], small["z"], small["iters"]
+        S0s = O.init_S(Xs, zs, 0)
+        reps, t_all = 0, 0.0
+        while t_all < 1.0 and reps < 200:
+            t0 = time.perf_counter()
+            O.bld_mult(Xs, zs, small["alpha"], small["beta"], it, O.PSI_APPR, 1e-50, S0=S0s)
+            t_all += time.perf_counter() - t0
+            reps += 1
+        out["plain_64x48x8"] = {"ms_per_solve": t_all * 1e3 / reps,
+                                "value": Xs.size * zs * it * reps / t_all,
+                                "unit": "S-updates/s", "iters": it, "solves_timed": reps}
+    return out
 
 
 def dist_setup():
@@ -192,7 +233,7 @@ def run_reference(args):
                        "iters_per_step": per_step, "psi": "psi_appr", "storage": "f64",
                        "parallelism": "host threads"},
             "cpu_baseline": {"value": value, "unit": "S-updates/s", "cores": cores,
-                             "kind": "port",
+                             "kind": "port", "cpu_model": cpu_model(), "nproc": os.cpu_count(),
                              "sample": f"{per_step} iteration(s) of the full 1024x1024x64 "
                                        "workload per step; the reference is not buildable here "
                                        "(Eigen3/GSL absent), its OpenMP restatement runs"},
@@ -267,6 +308,216 @@ def run_sharded(args):
     return 0
 
 
+def plain_measure(pkg, torch, prob, f64, steps, warmup, dev, stream, dist, world,
+                  with_skip=True, with_e2e_S0=True):
+    """The plain solve of `prob` on one device: device-resident rate, roofline of
+    the update sweep, the skip_zero_rows variant and the drop-in host-buffer e2e.
+    Returns (result dict, plan, dX, dS) with the plan still open."""
+    X, z, iters = prob["X"], prob["z"], prob["iters"]
+    x, y = X.shape
+    dt_t = torch.float64 if f64 else torch.float32
+    dtype = pkg.F64 if f64 else pkg.F32
+    es = 8 if f64 else 4
+    dtn = "f64" if f64 else "f32"
+    dX = torch.as_tensor(X).to(dev, dt_t)
+    dalpha = torch.as_tensor(prob["alpha"]).to(dev)
+    dbeta = torch.as_tensor(prob["beta"]).to(dev)
+    dS = torch.empty((x, y, z), dtype=dt_t, device=dev)
+    plan = pkg.Plan(x, y, z, dtype)
+    plan.init_S(dX, dS, seed=0)
+    mode = pkg.PSI_APPR
+
+    def step():
+        plan.run(dX, dalpha, dbeta, dS, iters, mode, 1e-50, stream)
+
+    for _ in range(warmup):
+        step()
+    plan.check(stream)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = plan.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index or 0) as clk:
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = plan.launch_count() - launches0
+    plan.check(stream)
+    ms = e0.elapsed_time(e1) / steps
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if dist:
+        dist.barrier()
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    upd_step = x * y * z * iters
+    value = upd_step * world / (ms_max / 1e3)
+    conservation = plan.conservation(dX, dS, stream)
+
+    # Roofline of the fused update sweep: CUDA events around each launch.
+    kern_ms, iter_ms = plan.profile(dX, dalpha, dbeta, dS, 20, mode, 1e-50, stream)
+    alg_bytes = 2 * x * y * z * es + x * y * es
+    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+    peak, peak_src = hbm_peak()
+    prof = f"sweep_update_plain_{x}x{y}x{z}_{dtn}.md"
+    traffic, traffic_src = profile_value(prof)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src,
+                "traffic": traffic, "traffic_source": traffic_src,
+                "kernel_source_sha": kernel_source_sha(),
+                "kernel": "sweep_kernel<UPDATE>", "kernel_ms": kern_ms,
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "iteration_ms": iter_ms,
+                "iteration_frac": alg_bytes / (iter_ms / 1e3) / 1e9 / peak}
+    # The secondary ceiling: FP64 arithmetic of the same launch (flops counted by
+    # ncu on the committed capture of this workload, 2*DFMA + DADD + DMUL).
+    fp64 = None
+    flop, flop_src = profile_value(prof, "fp64_flop_per_launch")
+    if flop and f64:
+        fp64 = {"flop_per_launch": flop, "flop_source": flop_src,
+                "achieved_tflops": flop / (kern_ms / 1e3) / 1e12,
+                "peak_tflops": FP64_NOMINAL_TFLOPS, "peak_source": "nominal",
+                "frac": flop / (kern_ms / 1e3) / 1e12 / FP64_NOMINAL_TFLOPS}
+
+    zero_row_skip = None
+    if with_skip:
+        # The same solve with skip_zero_rows: bitwise the same S; after the first
+        # update, rows whose band segment of X is all zero are neither read nor
+        # written and zeros are not stored again.  Its rate counts all x*y*z
+        # updates of an iteration; the roofline above stays the streaming kernel's.
+        plan_skip = pkg.Plan(x, y, z, dtype, skip_zero_rows=True)
+        dS2 = torch.empty_like(dS)
+        plan_skip.init_S(dX, dS2, seed=0)
+        for _ in range(2):
+            plan_skip.run(dX, dalpha, dbeta, dS2, iters, mode, 1e-50, stream)
+        plan_skip.check(stream)
+        n_skip = max(1, steps // 3)
+        e0.record(stream)
+        for _ in range(n_skip):
+            plan_skip.run(dX, dalpha, dbeta, dS2, iters, mode, 1e-50, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plan_skip.check(stream)
+        skip_ms = e0.elapsed_time(e1) / n_skip
+        skip_kern, _ = plan_skip.profile(dX, dalpha, dbeta, dS2, 20, mode, 1e-50, stream)
+        zero_row_skip = {"value": upd_step / (skip_ms / 1e3), "unit": "S-updates/s",
+                         "ms_per_step": skip_ms, "speedup": ms_max / skip_ms,
+                         "update_kernel_ms": skip_kern, "steps": n_skip,
+                         "fibers_with_X_nonzero": float(np.mean(X != 0)),
+                         "note": "bldm_tuning.skip_zero_rows; bitwise the same S"}
+        plan_skip.close()
+        del dS2
+
+    # End to end through the public host-buffer C ABI, as the drop-in call
+    # bld_mult_cuda(X, z, params, max_iter, true) makes it: pinned host X in,
+    # the seeded initial S drawn on the device, S out (H2D of X, alpha, beta and
+    # D2H of S inside every step).  A second measurement passes a host S0 as
+    # well (its H2D inside the step).
+    hX = torch.as_tensor(X.astype(np.float64 if f64 else np.float32)).pin_memory()
+    hS0 = dS.cpu().pin_memory()
+    hS = torch.empty_like(hS0).pin_memory()
+    params = pkg.Params(prob["a"], prob["b"], prob["alpha"], prob["beta"])
+    cp = params.c_struct()
+    L = pkg.lib()
+    solve = L.bldm_solve_f64 if f64 else L.bldm_solve_f32
+    ptr_t = ctypes.POINTER(ctypes.c_double if f64 else ctypes.c_float)
+    st = pkg.bldm_stats()
+
+    def e2e_step(with_S0):
+        s0 = ctypes.cast(hS0.data_ptr(), ptr_t) if with_S0 else None
+        rc = solve(ctypes.cast(hX.data_ptr(), ptr_t), x, y, z, ctypes.byref(cp), iters, mode,
+                   1e-50, s0, 0, ctypes.cast(hS.data_ptr(), ptr_t), ctypes.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"bldm_solve failed with status {rc}")
+
+    def e2e_time(with_S0, n):
+        for _ in range(max(1, warmup)):
+            e2e_step(with_S0)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            e2e_step(with_S0)
+        sec = (time.perf_counter() - t0) / n
+        t = torch.tensor([sec], device=dev, dtype=torch.float64)
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    e2e_s = e2e_time(False, steps)
+    h2d = x * y * es + (x + z) * 8
+    d2h = x * y * z * es
+    e2e = {"value": upd_step * world / e2e_s, "unit": "S-updates/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
+           "conservation_residual_last_call": st.conservation_residual,
+           "call": f"bldm_solve_{dtn} (host X in, device-seeded S0, host S out)"}
+    e2e_from_S0 = None
+    if with_e2e_S0:
+        e2e_s0_s = e2e_time(True, max(1, steps // 3))
+        e2e_from_S0 = {"value": upd_step * world / e2e_s0_s, "unit": "S-updates/s",
+                       "h2d_bytes_per_step": h2d + x * y * z * es, "d2h_bytes_per_step": d2h,
+                       "ms_per_step": e2e_s0_s * 1e3}
+    res = {"value": value, "ms_per_step": ms_max, "launches": launches,
+           "upd_step": upd_step, "alg_bytes": alg_bytes,
+           "hbm_gbs_iteration": alg_bytes / (ms_max / 1e3 / iters) / 1e9,
+           "roofline": roofline, "fp64_arith": fp64, "zero_row_skip": zero_row_skip,
+           "e2e": e2e, "e2e_from_host_S0": e2e_from_S0, "clocks": clk.summary(),
+           "conservation_residual": conservation}
+    return res, plan, dX, dS
+
+
+def parity_block(pkg, torch, prob, dS64, plan64, stream):
+    """Parity of this build on the benchmark's own inputs, measured in the run:
+    (1) the CPU-runnable 64x48x8 workload, 200 iterations through the drop-in
+    call against the oracle (max-norm relative error of S); (2) the timed
+    solve's conservation residual (filled in by the caller); (3) FP32 storage
+    against FP64 on the headline workload from the same initial S, 100
+    iterations: log-marginal gap and S error."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import bnmf_algs_b200.workloads as W
+    small = W.plain_small(0)
+    Xs, zs = small["X"], small["z"]
+    S0s = O.init_S(Xs, zs, 0)
+    ref = O.bld_mult(Xs, zs, small["alpha"], small["beta"], small["iters"], O.PSI_APPR, 1e-50,
+                     S0=S0s)
+    ps = pkg.Params(small["a"], small["b"], small["alpha"], small["beta"])
+    got = pkg.bld_mult_cuda(Xs, zs, ps, small["iters"], use_psi_appr=True, S0=S0s)
+    err_small = float(np.abs(got - ref).max() / max(np.abs(ref).max(), 1e-300))
+    # FP32 vs FP64 on the headline workload from one initial S
+    X, z, iters = prob["X"], prob["z"], prob["iters"]
+    x, y = X.shape
+    dX64 = torch.as_tensor(X).cuda()
+    da = torch.as_tensor(prob["alpha"]).cuda()
+    db = torch.as_tensor(prob["beta"]).cuda()
+    S64 = torch.empty((x, y, z), dtype=torch.float64, device="cuda")
+    plan64.init_S(dX64, S64, seed=7, stream=stream)
+    S32 = S64.float()
+    p32 = pkg.Plan(x, y, z, pkg.F32)
+    plan64.run(dX64, da, db, S64, iters, pkg.PSI_APPR, 1e-50, stream)
+    p32.run(dX64.float(), da, db, S32, iters, pkg.PSI_APPR, 1e-50, stream)
+    plan64.check(stream)
+    p32.check(stream)
+    params = pkg.Params(prob["a"], prob["b"], prob["alpha"], prob["beta"])
+    lm64 = pkg.log_marginal_S(S64, params, stream=stream)
+    lm32 = pkg.log_marginal_S(S32, params, dtype=pkg.F32, stream=stream)
+    mask = S64 > 1e-6 * dX64.unsqueeze(2)
+    rel = ((S32.double() - S64).abs() / S64.abs().clamp_min(1e-300))[mask]
+    p32.close()
+    out = {"plain_64x48x8_fp64_max_rel_err_S_vs_oracle": err_small,
+           "plain_64x48x8_iters": small["iters"], "plain_64x48x8_tolerance": 1e-9,
+           "fp32_vs_fp64_log_marginal_rel_gap": abs(lm32 - lm64) / abs(lm64),
+           "fp32_vs_fp64_log_marginal_tolerance": 1e-5,
+           "fp32_vs_fp64_max_rel_err_S": float(rel.max()) if rel.numel() else 0.0,
+           "fp32_vs_fp64_median_rel_err_S": float(rel.median()) if rel.numel() else 0.0,
+           "fp32_vs_fp64_workload": f"{x}x{y}x{z}, {iters} iterations from one initial S "
+                                    "(S error over S > 1e-6 X)"}
+    del S64, S32, dX64
+    return out
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_setup()
@@ -283,163 +534,64 @@ def run_ours(args):
     X, z, iters = prob["X"], prob["z"], prob["iters"]
     x, y = X.shape
     f64 = args.dtype == "f64"
-    dt_t = torch.float64 if f64 else torch.float32
-    dtype = pkg.F64 if f64 else pkg.F32
-    es = 8 if f64 else 4
     dev = torch.device("cuda", local)
-    dX = torch.as_tensor(X).to(dev, dt_t)
-    dalpha = torch.as_tensor(prob["alpha"]).to(dev)
-    dbeta = torch.as_tensor(prob["beta"]).to(dev)
-    dS = torch.empty((x, y, z), dtype=dt_t, device=dev)
-    plan = pkg.Plan(x, y, z, dtype)
-    plan.init_S(dX, dS, seed=0)
-    mode = pkg.PSI_APPR
     stream = torch.cuda.current_stream()
-
-    def step():
-        plan.run(dX, dalpha, dbeta, dS, iters, mode, 1e-50, stream)
-
-    for _ in range(args.warmup):
-        step()
-    plan.check(stream)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = plan.launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-    launches = plan.launch_count() - launches0
-    plan.check(stream)
-    ms = e0.elapsed_time(e1) / args.steps
-    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if dist:
-        dist.barrier()
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    upd_step = x * y * z * iters
-    value = upd_step * world / (ms_max / 1e3)
-
-    # Roofline of the fused update sweep: CUDA events around each launch.
-    kern_ms, iter_ms = plan.profile(dX, dalpha, dbeta, dS, 20, mode, 1e-50, stream)
-    alg_bytes = 2 * x * y * z * es + x * y * es
-    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
-    peak, peak_src = hbm_peak()
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_src,
-                "traffic": profile_traffic(f"sweep_update_plain_1024x1024x64_{args.dtype}.md"),
-                "kernel": "sweep_kernel<UPDATE>", "kernel_ms": kern_ms,
-                "algorithmic_bytes_per_launch": alg_bytes,
-                "iteration_ms": iter_ms,
-                "iteration_frac": alg_bytes / (iter_ms / 1e3) / 1e9 / peak}
-    # The secondary ceiling: FP64 arithmetic of the same launch (flops counted by ncu on the
-    # committed profile of this workload, 2*DFMA + DADD + DMUL thread instructions).
-    flop = profile_value(f"sweep_update_plain_1024x1024x64_{args.dtype}.md", "fp64_flop_per_launch")
-    fp64 = None
-    if flop and args.dtype == "f64" and (x, y, z) == (1024, 1024, 64):
-        fp64 = {"flop_per_launch": flop, "achieved_tflops": flop / (kern_ms / 1e3) / 1e12,
-                "peak_tflops": FP64_NOMINAL_TFLOPS, "peak_source": "nominal",
-                "frac": flop / (kern_ms / 1e3) / 1e12 / FP64_NOMINAL_TFLOPS}
-
-    # The same solve with skip_zero_rows: bitwise the same S; after the first
-    # update, rows whose band segment of X is all zero are neither read nor
-    # written and zeros are not stored again.  Its rate counts all x*y*z
-    # updates of an iteration; the roofline above stays the streaming kernel's.
-    plan_skip = pkg.Plan(x, y, z, dtype, skip_zero_rows=True)
-    dS2 = torch.empty_like(dS)
-    plan_skip.init_S(dX, dS2, seed=0)
-    for _ in range(2):
-        plan_skip.run(dX, dalpha, dbeta, dS2, iters, mode, 1e-50, stream)
-    plan_skip.check(stream)
-    n_skip = max(1, args.steps // 3)
-    e0.record(stream)
-    for _ in range(n_skip):
-        plan_skip.run(dX, dalpha, dbeta, dS2, iters, mode, 1e-50, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    plan_skip.check(stream)
-    skip_ms = e0.elapsed_time(e1) / n_skip
-    skip_kern, _ = plan_skip.profile(dX, dalpha, dbeta, dS2, 20, mode, 1e-50, stream)
-    zero_row_skip = {"value": upd_step / (skip_ms / 1e3), "unit": "S-updates/s",
-                     "ms_per_step": skip_ms, "speedup": ms_max / skip_ms,
-                     "update_kernel_ms": skip_kern, "steps": n_skip,
-                     "fibers_with_X_nonzero": float(np.mean(X != 0)),
-                     "note": "bldm_tuning.skip_zero_rows; bitwise the same S"}
-    plan_skip.close()
-    del dS2
-
-    # End to end through the public host-buffer C ABI, as the drop-in call
-    # bld_mult_cuda(X, z, params, max_iter, true) makes it: pinned host X in,
-    # the seeded initial S drawn on the device, S out (H2D of X, alpha, beta
-    # and D2H of S inside every step).  A second measurement passes a host S0
-    # as well (its H2D inside the step).
-    hX = torch.as_tensor(X.astype(np.float64 if f64 else np.float32)).pin_memory()
-    hS0 = dS.cpu().pin_memory()
-    hS = torch.empty_like(hS0).pin_memory()
-    params = pkg.Params(prob["a"], prob["b"], prob["alpha"], prob["beta"])
-    cp = params.c_struct()
-    L = pkg.lib()
-    solve = L.bldm_solve_f64 if f64 else L.bldm_solve_f32
-    ptr_t = ctypes.POINTER(ctypes.c_double if f64 else ctypes.c_float)
-
-    def e2e_step(with_S0):
-        s0 = ctypes.cast(hS0.data_ptr(), ptr_t) if with_S0 else None
-        rc = solve(ctypes.cast(hX.data_ptr(), ptr_t), x, y, z, ctypes.byref(cp), iters, mode,
-                   1e-50, s0, 0, ctypes.cast(hS.data_ptr(), ptr_t), None)
-        if rc != 0:
-            raise RuntimeError(f"bldm_solve failed with status {rc}")
-
-    def e2e_time(with_S0, steps):
-        for _ in range(max(1, args.warmup)):
-            e2e_step(with_S0)
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            e2e_step(with_S0)
-        sec = (time.perf_counter() - t0) / steps
-        t = torch.tensor([sec], device=dev, dtype=torch.float64)
-        if dist:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    e2e_s = e2e_time(False, args.steps)
-    e2e_value = upd_step * world / e2e_s
-    h2d = x * y * es + (x + z) * 8
-    d2h = x * y * z * es
-    e2e_s0_s = e2e_time(True, max(1, args.steps // 3))
-    e2e_from_S0 = {"value": upd_step * world / e2e_s0_s, "unit": "S-updates/s",
-                   "h2d_bytes_per_step": h2d + x * y * z * es, "d2h_bytes_per_step": d2h,
-                   "ms_per_step": e2e_s0_s * 1e3}
-
+    head, plan, dX, dS = plain_measure(pkg, torch, prob, f64, args.steps, args.warmup, dev,
+                                       stream, dist, world)
+    # The extra blocks are one-GPU measurements of the other benchmark workloads;
+    # with several ranks only the headline replicas run.
+    extra = world == 1 and not args.headline_only
+    parity = fp32 = batch = serving = None
+    if extra:
+        parity = parity_block(pkg, torch, prob, dS, plan, stream)
+        parity["headline_conservation_residual"] = head["conservation_residual"]
+        parity["headline_e2e_conservation_residual"] = head["e2e"][
+            "conservation_residual_last_call"]
+    plan.close()
+    del dX, dS
+    torch.cuda.empty_cache()
+    if extra and f64:
+        r32, p32, dX32, dS32 = plain_measure(pkg, torch, prob, False, args.steps, args.warmup,
+                                             dev, stream, None, 1, with_skip=False,
+                                             with_e2e_S0=False)
+        p32.close()
+        del dX32, dS32
+        torch.cuda.empty_cache()
+        fp32 = {"value": r32["value"], "unit": "S-updates/s", "ms_per_step": r32["ms_per_step"],
+                "roofline": r32["roofline"], "e2e": r32["e2e"],
+                "conservation_residual": r32["conservation_residual"],
+                "vs_fp64_plain": r32["value"] / head["value"], "gpu_launches": r32["launches"],
+                "clocks": r32["clocks"]}
+    if extra:
+        batch = batch_measure(pkg, torch, args, steps=max(3, args.steps // 3), loop_reps=1)
+        batch["vs_plain_fp64_S_updates_per_s"] = batch["S_updates_per_s"] / head["value"]
+        if fp32:
+            batch["vs_plain_fp32_S_updates_per_s"] = batch["S_updates_per_s"] / fp32["value"]
+        torch.cuda.empty_cache()
+        serving = serve_measure(pkg, torch, args.serve_sample_rate, args.serve_sample_seconds,
+                                fp64_sample=4, dtype_name="f32")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_oracle(prob, target_s=args.cpu_seconds)
+        cpu = cpu_baseline_oracle(prob, target_s=args.cpu_seconds, small=W.plain_small(0))
 
     if rank == 0:
-        line = {"metric": "S_elem_updates_per_s", "value": value, "unit": "S-updates/s",
+        line = {"metric": "S_elem_updates_per_s", "value": head["value"], "unit": "S-updates/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
                 "config": {"workload": "plain_1024x1024x64", "x": x, "y": y, "z": z,
                            "iters_per_step": iters, "psi": "psi_appr", "storage": args.dtype,
                            "X_zero_fraction": float(np.mean(X == 0)),
                            "l2": "inputs larger than L2 (S is 512 MiB in f64)",
                            "parallelism": "replicas" if world > 1 else "single GPU"},
-                "hbm_gbs_iteration": alg_bytes / (ms_max / 1e3 / iters) / 1e9,
-                "roofline": roofline, "fp64_arith": fp64, "zero_row_skip": zero_row_skip,
-                "cpu_baseline": cpu,
-                "e2e": {"value": e2e_value, "unit": "S-updates/s", "h2d_bytes_per_step": h2d,
-                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
-                        "call": "bldm_solve (host X in, device-seeded S0, host S out)"},
-                "e2e_from_host_S0": e2e_from_S0,
-                "gpu_launches": launches, "clocks": clk.summary()}
+                "hbm_gbs_iteration": head["hbm_gbs_iteration"],
+                "roofline": head["roofline"], "fp64_arith": head["fp64_arith"],
+                "zero_row_skip": head["zero_row_skip"],
+                "cpu_baseline": cpu, "e2e": head["e2e"],
+                "e2e_from_host_S0": head["e2e_from_host_S0"],
+                "gpu_launches": head["launches"], "clocks": head["clocks"],
+                "parity": parity, "fp32_plain": fp32, "batch": batch, "serving": serving}
         print(json.dumps(line))
-    plan.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -495,14 +647,14 @@ def run_batch_probe(args):
     return 0
 
 
-def run_batch(args):
-    """Batched uneven solves vs looping the plain per-instance solver."""
-    import torch
-    pkg = load_package()
+def batch_measure(pkg, torch, args, steps, loop_reps=2, autotune=True):
+    """Batched uneven solves (512 instances, FP32 unless --dtype f64, 150
+    iterations, one graph-captured run per step) against a loop of the plain
+    per-instance solver over the same instances."""
     import bnmf_algs_b200.workloads as W
     shapes = W.batch_shapes(args.batch_n, 3)
     iters = 150
-    f64 = args.dtype == "f64"
+    f64 = args.batch_dtype == "f64"
     dtype = pkg.F64 if f64 else pkg.F32
     es = 8 if f64 else 4
     upd = sum(x * y * z for x, y, z in shapes) * iters
@@ -516,7 +668,7 @@ def run_batch(args):
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.Stream()
     tune = None
-    if not args.no_autotune:
+    if autotune:
         t1 = time.perf_counter()
         d_ms, t_ms = b.autotune(probe_iters=3, psi_mode=pkg.PSI_APPR, eps=1e-50, stream=stream)
         tune = {"seconds": time.perf_counter() - t1, "probe_iters": 3,
@@ -531,82 +683,99 @@ def run_batch(args):
     l0 = b.info()["launches"]
     with ClockSampler(0) as clk:
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             b.run(iters, pkg.PSI_APPR, 1e-50, True, stream)
         e1.record(stream)
         torch.cuda.synchronize()
     b.check(stream)
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = e0.elapsed_time(e1) / steps
     launches = b.info()["launches"] - l0
+    cons = b.conservation(stream)
     # loop of the plain per-instance solver (one plan per distinct shape)
     plans = {}
     dev = []
+    tt = torch.float64 if f64 else torch.float32
     for (x, y, z), pr in zip(shapes, probs):
         if (x, y, z) not in plans:
             plans[(x, y, z)] = pkg.Plan(x, y, z, dtype)
-        tt = torch.float64 if f64 else torch.float32
         dX = torch.as_tensor(pr["X"]).to("cuda", tt)
         dS = torch.empty((x, y, z), dtype=tt, device="cuda")
         plans[(x, y, z)].init_S(dX, dS, seed=0)
         dev.append((plans[(x, y, z)], dX, torch.as_tensor(pr["alpha"]).cuda(),
                     torch.as_tensor(pr["beta"]).cuda(), dS))
+
     def loop():
         for plan, dX, da, db, dS in dev:
             plan.run(dX, da, db, dS, iters, pkg.PSI_APPR, 1e-50, stream)
     loop()
     torch.cuda.synchronize()
     e0.record(stream)
-    loop()
+    for _ in range(loop_reps):
+        loop()
     e1.record(stream)
     torch.cuda.synchronize()
-    loop_ms = e0.elapsed_time(e1)
+    loop_ms = e0.elapsed_time(e1) / loop_reps
+    for p in plans.values():
+        p.close()
+    del dev
     alg_bytes = sum(2 * x * y * z * es + x * y * es for x, y, z in shapes) * iters
     peak, _ = hbm_peak()
-    line = {"metric": "batched_solves_per_s", "value": len(shapes) / (ms / 1e3),
-            "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": args.dtype, "data": "synthetic",
-            "config": {"workload": f"batch_{len(shapes)}_uneven", "iters": iters,
-                       "x_y": "log-uniform [32,512]", "z": "{4,8,16,32,64}",
-                       "total_S_elements": sum(x * y * z for x, y, z in shapes),
-                       "rows_per_tile": "autotuned per class" if tune else
-                       (args.rows_per_tile or 64), "graph": True},
-            "S_updates_per_s": upd / (ms / 1e3),
-            "hbm_gbs_algorithmic": alg_bytes / (ms / 1e3) / 1e9,
-            "frac_of_hbm_peak": alg_bytes / (ms / 1e3) / 1e9 / peak,
-            "plain_loop": {"ms": loop_ms, "solves_per_s": len(shapes) / (loop_ms / 1e3),
-                           "S_updates_per_s": upd / (loop_ms / 1e3)},
-            "speedup_vs_plain_loop": loop_ms / ms,
-            "classes": b.info()["classes"], "gpu_launches": launches,
-            "setup_s": setup_s, "autotune": tune, "clocks": clk.summary()}
-    print(json.dumps(line))
+    out = {"metric": "batched_solves_per_s", "value": len(shapes) / (ms / 1e3),
+           "unit": "solves/s", "ms_per_step": ms, "steps": steps, "dtype": args.batch_dtype,
+           "config": {"workload": f"batch_{len(shapes)}_uneven", "iters": iters,
+                      "x_y": "log-uniform [32,512]", "z": "{4,8,16,32,64}",
+                      "total_S_elements": sum(x * y * z for x, y, z in shapes),
+                      "rows_per_tile": "autotuned per class" if tune else
+                      (args.rows_per_tile or 64), "graph": True},
+           "S_updates_per_s": upd / (ms / 1e3),
+           "hbm_gbs_algorithmic": alg_bytes / (ms / 1e3) / 1e9,
+           "frac_of_hbm_peak": alg_bytes / (ms / 1e3) / 1e9 / peak,
+           "plain_loop": {"ms": loop_ms, "solves_per_s": len(shapes) / (loop_ms / 1e3),
+                          "S_updates_per_s": upd / (loop_ms / 1e3)},
+           "speedup_vs_plain_loop": loop_ms / ms,
+           "conservation_residual_max": float(np.max(cons)),
+           "conservation_residual_median": float(np.median(cons)),
+           "classes": b.info()["classes"], "gpu_launches": launches,
+           "gpu_launches_per_solve_iteration": launches / (steps * iters),
+           "setup_s": setup_s, "autotune": tune, "clocks": clk.summary()}
     b.close()
+    return out
+
+
+def run_batch(args):
+    import torch
+    pkg = load_package()
+    out = batch_measure(pkg, torch, args, args.steps)
+    line = {"metric": out.pop("metric"), "value": out.pop("value"), "unit": out.pop("unit"),
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic"}
+    line.update(out)
+    print(json.dumps(line))
     return 0
 
 
-def run_serve(args):
-    """Continuous-batching server under Poisson arrivals."""
-    import threading
-    import torch
-    pkg = load_package()
+def serve_measure(pkg, torch, rate, duration, fp64_sample=16, dtype_name="f32"):
+    """Continuous-batching server under Poisson arrivals at `rate` req/s for
+    `duration` s of traffic: latency percentiles, throughput, and per-request
+    log-marginal error against an FP64 solve of the same request."""
+    import queue as _queue
     import bnmf_algs_b200.workloads as W
     rng = np.random.default_rng(11)
     # request templates: the batch size distribution plus the 4096x4096x32 tail
     reg = [W.batch_instance(s, 5000 + k) for k, s in enumerate(W.batch_shapes(96, 21))]
     tail = [W.batch_instance((4096, 4096, 32), 9000 + k) for k in range(2)]
-    n_max = int(args.rate * args.duration * 1.5) + 16
-    times, _ = W.serving_requests(n_max, args.rate, seed=4)
-    times = times[times < args.duration]
+    n_max = int(rate * duration * 1.5) + 16
+    times, _ = W.serving_requests(n_max, rate, seed=4)
+    times = times[times < duration]
     picks = []
     for _ in range(len(times)):
         picks.append(tail[rng.integers(len(tail))] if rng.random() < 0.02
                      else reg[rng.integers(len(reg))])
-    dtype = pkg.F64 if args.dtype == "f64" else pkg.F32
+    dtype = pkg.F64 if dtype_name == "f64" else pkg.F32
     srv = pkg.Server(dtype=dtype, tol=1e-6, max_iter=500, iters_per_round=10, max_active=256)
-    import queue as _queue
     pending = _queue.Queue()
     results = []
-    n_keep_S = args.fp64_sample
+    n_keep_S = fp64_sample
 
     def consume():
         # fetches in submission order as results complete; S only for the
@@ -644,10 +813,11 @@ def run_serve(args):
     tail_lat = np.array([r[3]["latency_ms"] for r in ok if r[1]["X"].shape == (4096, 4096)])
     reg_lat = np.array([r[3]["latency_ms"] for r in ok if r[1]["X"].shape != (4096, 4096)])
     iters = np.array([r[3]["iterations"] for r in ok])
+    cons = np.array([r[3]["conservation_residual"] for r in ok])
     upd = sum(r[1]["X"].size * r[1]["z"] * r[3]["iterations"] for r in ok)
     # per-request log-marginal error vs an FP64 solve of the same request
     errs = []
-    sample = [r for r in ok if r[2] is not None][: args.fp64_sample]
+    sample = [r for r in ok if r[2] is not None][:fp64_sample]
     for k, pr, S, st in sample:
         x, y = pr["X"].shape
         z = pr["z"]
@@ -662,24 +832,35 @@ def run_serve(args):
         errs.append(abs(st["log_marginal"] - lm64) / abs(lm64))
         plan.close()
     pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None
-    line = {"metric": "serving_latency_p50_p99", "value": pct(lat, 50), "unit": "ms (p50)",
-            "p99_ms": pct(lat, 99), "n_gpus": 1, "higher_is_better": False,
-            "dtype": args.dtype, "data": "synthetic",
-            "config": {"workload": "serving_poisson", "offered_rate_per_s": args.rate,
-                       "duration_s": args.duration, "tol": 1e-6, "max_iter": 500,
+    return {"metric": "serving_latency_p50_p99", "value": pct(lat, 50), "unit": "ms (p50)",
+            "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "higher_is_better": False,
+            "dtype": dtype_name,
+            "config": {"workload": "serving_poisson", "offered_rate_per_s": rate,
+                       "duration_s": duration, "tol": 1e-6, "max_iter": 500,
                        "iters_per_round": 10, "sizes": "batch distribution + 2% 4096x4096x32"},
             "requests": len(results), "completed": len(ok), "solves_per_s": len(ok) / wall,
             "S_updates_per_s": upd / wall, "wall_s": wall,
             "regular_p50_ms": pct(reg_lat, 50), "regular_p99_ms": pct(reg_lat, 99),
             "tail_requests": int(len(tail_lat)), "tail_p50_ms": pct(tail_lat, 50),
-            "iterations_p50": pct(iters, 50), "iterations_max": int(iters.max()) if len(iters) else 0,
+            "iterations_p50": pct(iters, 50),
+            "iterations_max": int(iters.max()) if len(iters) else 0,
+            "conservation_residual_max": float(cons.max()) if len(cons) else None,
             "log_marginal_rel_err_vs_fp64": {"max": max(errs) if errs else None,
                                              "median": float(np.median(errs)) if errs else None,
                                              "n": len(errs)},
             "gpu_busy_frac": sstats["gpu_ms"] / 1e3 / wall,
-            "gpu_busy_frac_lanes": {"small": (sstats["gpu_ms"] - sstats["gpu_ms_large"]) / 1e3 / wall,
-                                    "large": sstats["gpu_ms_large"] / 1e3 / wall},
+            "gpu_busy_frac_lanes": {"small": (sstats["gpu_ms"] - sstats["gpu_ms_large"]) / 1e3
+                                    / wall, "large": sstats["gpu_ms_large"] / 1e3 / wall},
             "server": sstats, "clocks": clk.summary()}
+
+
+def run_serve(args):
+    import torch
+    pkg = load_package()
+    out = serve_measure(pkg, torch, args.rate, args.duration, args.fp64_sample, args.dtype)
+    line = {"metric": out.pop("metric"), "value": out.pop("value"), "unit": out.pop("unit"),
+            "n_gpus": 1, "data": "synthetic"}
+    line.update(out)
     print(json.dumps(line))
     return 0
 
@@ -739,7 +920,8 @@ def run_precision(args):
         p32.close()
     line = {"metric": "precision_fp32_vs_fp64", "dtype": "f32 vs f64", "data": "synthetic",
             "config": {"workload": "precision_2048x2048x32", "iters": base["iters"],
-                       "X": "Poisson(rate_i), rate_i~LogNormal(0,1.5), 30% zeros",
+                       "X": "30% zeros; otherwise Poisson(rate_i) conditioned on >= 1, "
+                            "rate_i~LogNormal(0,1.5)",
                        "zero_fraction": float(np.mean(X == 0))},
             "results": out}
     print(json.dumps(line))
@@ -819,6 +1001,12 @@ def main():
                     help="batched uneven solves: 512 instances, x,y log-uniform in [32,512], "
                          "z in {4..64}, FP32, 150 iterations; vs a loop of the plain solver")
     ap.add_argument("--batch-n", type=int, default=512)
+    ap.add_argument("--headline-only", action="store_true",
+                    help="default mode: skip the parity, FP32, batch and serving blocks")
+    ap.add_argument("--serve-sample-rate", type=float, default=50.0,
+                    help="offered rate (req/s) of the default run's serving sample")
+    ap.add_argument("--serve-sample-seconds", type=float, default=12.0,
+                    help="seconds of traffic of the default run's serving sample")
     ap.add_argument("--sharded", action="store_true",
                     help="the headline solve row-sharded over the torchrun ranks (NCCL)")
     ap.add_argument("--batch-probe", action="store_true",
@@ -845,6 +1033,8 @@ def main():
         args.warmup = 3
     if args.dtype is None:
         args.dtype = "f32" if (args.batch or args.serve or args.batch_probe) else "f64"
+    # the default run's batch block is the FP32-compensated batched form
+    args.batch_dtype = args.dtype if (args.batch or args.batch_probe) else "f32"
     if args.batch_probe:
         return run_batch_probe(args)
     if args.sharded:

@@ -69,7 +69,7 @@ class bldm_tuning(ctypes.Structure):
 class bldm_stats(ctypes.Structure):
     _fields_ = [("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("iterations", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
-                ("rel_change", ctypes.c_double)]
+                ("rel_change", ctypes.c_double), ("conservation_residual", ctypes.c_double)]
 
 
 class bldm_server_config(ctypes.Structure):
@@ -83,7 +83,8 @@ class bldm_server_config(ctypes.Structure):
 class bldm_request_stats(ctypes.Structure):
     _fields_ = [("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
                 ("iterations", ctypes.c_uint64), ("rel_change", ctypes.c_double),
-                ("log_marginal", ctypes.c_double), ("status", ctypes.c_int)]
+                ("log_marginal", ctypes.c_double), ("status", ctypes.c_int),
+                ("conservation_residual", ctypes.c_double)]
 
 
 class bldm_server_stats(ctypes.Structure):
@@ -148,6 +149,7 @@ SIGNATURES = {
     "bldm_plan_run": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _sz, ctypes.c_int, ctypes.c_double,
                                      _vp]),
     "bldm_plan_check": (ctypes.c_int, [_vp, _vp]),
+    "bldm_plan_conservation": (ctypes.c_int, [_vp, _vp, _vp, _vp, _dp]),
     "bldm_solve_device_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int,
                                                  _sz, ctypes.c_int, ctypes.c_double, _vp]),
     "bldm_plan_init_S": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_uint64, _vp]),
@@ -191,6 +193,7 @@ SIGNATURES = {
                                       _vp]),
     "bldm_batch_check": (ctypes.c_int, [_vp, _vp]),
     "bldm_batch_get": (ctypes.c_int, [_vp, _sz, _dp, _dp]),
+    "bldm_batch_conservation": (ctypes.c_int, [_vp, _dp, _vp]),
     "bldm_batch_device_ptrs": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp),
                                               ctypes.POINTER(_vp)]),
     "bldm_batch_info": (ctypes.c_int, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz),
@@ -276,7 +279,8 @@ def _solve(X, z, params, max_iter, psi_mode, eps, S0, seed, dtype, stats):
     _check(rc, "bldm_solve")
     if stats is not None:
         stats.update(device_ms=st.device_ms, total_ms=st.total_ms, iterations=st.iterations,
-                     kernel_launches=st.kernel_launches)
+                     kernel_launches=st.kernel_launches,
+                     conservation_residual=st.conservation_residual)
     return out
 
 
@@ -358,6 +362,13 @@ class Plan:
 
     def check(self, stream=None):
         _check(lib().bldm_plan_check(self._h, _stream_ptr(stream)), "plan_check")
+
+    def conservation(self, dX, dS, stream=None):
+        """max_ij |sum_k S - X| / max(X, 1) of device tensors, computed on the device."""
+        out = ctypes.c_double()
+        _check(lib().bldm_plan_conservation(self._h, _ptr(dX), _ptr(dS), _stream_ptr(stream),
+                                            ctypes.byref(out)), "plan_conservation")
+        return out.value
 
     def init_S(self, dX, dS, seed=0, stream=None):
         _check(lib().bldm_plan_init_S(self._h, _ptr(dX), _ptr(dS), int(seed),
@@ -591,6 +602,13 @@ class Batch:
         _check(lib().bldm_batch_get(self._h, idx, S.ctypes.data_as(_dp), ctypes.byref(rel)))
         return S, rel.value
 
+    def conservation(self, stream=None):
+        """Row-sum conservation residual of every instance's current S (numpy array)."""
+        out = np.empty(len(self.shapes))
+        _check(lib().bldm_batch_conservation(self._h, out.ctypes.data_as(_dp),
+                                             _stream_ptr(stream)), "batch_conservation")
+        return out
+
     def info(self):
         nc, nb, nl = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_uint64()
         _check(lib().bldm_batch_info(self._h, ctypes.byref(nc), ctypes.byref(nb),
@@ -675,7 +693,8 @@ class Server:
                                      ctypes.byref(rs))
         stats = {"queue_ms": rs.queue_ms, "latency_ms": rs.latency_ms,
                  "iterations": rs.iterations, "rel_change": rs.rel_change,
-                 "log_marginal": rs.log_marginal, "status": rs.status}
+                 "log_marginal": rs.log_marginal, "status": rs.status,
+                 "conservation_residual": rs.conservation_residual}
         return (S if rc == OK else None), stats
 
     def cancel(self, rid):

@@ -20,9 +20,11 @@ struct bldm_batch {
     size_t arena_bytes = 0;
     int dtype = BLDM_F64;
     bool clean = false;  // every instance has been updated since its S was set
+    void* cons_buf = nullptr;  // conservation: ConsInst[n] | block_off[n+1] | residual bits[n]
     ~bldm_batch() {
         eng.reset();
         if (arena) cudaFree(arena);
+        if (cons_buf) cudaFree(cons_buf);
     }
 };
 
@@ -159,6 +161,48 @@ int bldm_batch_get(bldm_batch* b, size_t idx, double* S_out, double* rel_change)
     }
     if (rel_change) rc = cuda_status(cudaMemcpy(rel_change, in.rel, 8, cudaMemcpyDeviceToHost));
     return rc;
+}
+
+int bldm_batch_conservation(bldm_batch* b, double* residuals, void* stream) {
+    if (!b || !residuals) return BLDM_ERR_BAD_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t n = b->inst.size();
+    const size_t o_off = (n * sizeof(ConsInst) + 255) / 256 * 256;
+    const size_t o_out = (o_off + (n + 1) * sizeof(int) + 255) / 256 * 256;
+    const size_t bytes = o_out + n * sizeof(unsigned long long);
+    if (!b->cons_buf) {
+        const cudaError_t e = cudaMalloc(&b->cons_buf, bytes);
+        if (e != cudaSuccess) {
+            b->cons_buf = nullptr;
+            return cuda_status(e);
+        }
+    }
+    char* base = static_cast<char*>(b->cons_buf);
+    unsigned long long* d_out = reinterpret_cast<unsigned long long*>(base + o_out);
+    std::vector<char> host(bytes, 0);
+    ConsInst* ci = reinterpret_cast<ConsInst*>(host.data());
+    int* boff = reinterpret_cast<int*>(host.data() + o_off);
+    int blocks = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const EngineInstance& in = b->inst[i];
+        ci[i] = cons_inst(in.X, in.S, (long long)(in.x * in.y), (long long)in.z, d_out + i);
+        boff[i] = blocks;
+        blocks += conservation_blocks((long long)(in.x * in.y), (long long)in.z);
+    }
+    boff[n] = blocks;
+    int rc = cuda_status(cudaMemcpyAsync(base, host.data(), bytes, cudaMemcpyHostToDevice, st));
+    if (rc) return rc;
+    rc = launch_conservation_multi(b->dtype, reinterpret_cast<const ConsInst*>(base),
+                                   reinterpret_cast<const int*>(base + o_off), int(n), blocks, st);
+    if (rc) return rc;
+    std::vector<unsigned long long> bits(n);
+    rc = cuda_status(cudaMemcpyAsync(bits.data(), d_out, n * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, st));
+    if (rc) return rc;
+    rc = cuda_status(cudaStreamSynchronize(st));
+    if (rc) return rc;
+    for (size_t i = 0; i < n; ++i) residuals[i] = cons_value(bits[i]);
+    return BLDM_OK;
 }
 
 int bldm_batch_device_ptrs(bldm_batch* b, size_t idx, void** d_X, void** d_S) {

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "bldm_internal.h"
+#include "bldm_kernels.h"
 
 using namespace bldm;
 
@@ -221,6 +222,12 @@ int solve_impl(const T* X, size_t x, size_t y, size_t z, const bldm_params* para
         int r = run_iterations(e, max_iter, psi_mode, eps);
         if (r) return r;
         BLDM_CU_RET(cudaEventRecord(e->ev1, st));
+        // row-sum conservation of the result, one more read of S on the device
+        r = plan_conservation_launch(&e->plan, e->dX, e->dS, st);
+        if (r) return r;
+        unsigned long long cons_bits = 0;
+        BLDM_CU_RET(cudaMemcpyAsync(&cons_bits, e->plan.cons, sizeof cons_bits,
+                                    cudaMemcpyDeviceToHost, st));
         BLDM_CU_RET(cudaMemcpyAsync(S_out, e->dS, x * y * z * sizeof(T), cudaMemcpyDeviceToHost,
                                     st));
         r = plan_check(&e->plan, st);
@@ -231,6 +238,7 @@ int solve_impl(const T* X, size_t x, size_t y, size_t z, const bldm_params* para
             stats->device_ms = ms;
             stats->iterations = max_iter;
             stats->kernel_launches = e->plan.launches - launches0;
+            stats->conservation_residual = cons_value(cons_bits);
         }
         return BLDM_OK;
     };
@@ -331,6 +339,19 @@ int bldm_plan_run(bldm_plan* plan, const void* d_X, const double* d_alpha, const
     if (!plan) return BLDM_ERR_BAD_ARG;
     return plan_run(&plan->impl, d_X, d_alpha, d_beta, d_S, max_iter, psi_mode, eps,
                     static_cast<cudaStream_t>(stream), nullptr, 0);
+}
+
+int bldm_plan_conservation(bldm_plan* plan, const void* d_X, const void* d_S, void* stream,
+                           double* residual) {
+    if (!plan || !d_X || !d_S || !residual) return BLDM_ERR_BAD_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = plan_conservation_launch(&plan->impl, d_X, d_S, st);
+    if (rc) return rc;
+    unsigned long long bits = 0;
+    BLDM_CU_RET(cudaMemcpyAsync(&bits, plan->impl.cons, sizeof bits, cudaMemcpyDeviceToHost, st));
+    BLDM_CU_RET(cudaStreamSynchronize(st));
+    *residual = cons_value(bits);
+    return BLDM_OK;
 }
 
 int bldm_plan_check(bldm_plan* plan, void* stream) {

@@ -35,6 +35,16 @@ struct SweepCfg {
     int fin_threads;
 };
 
+// Byte offsets of the pieces of a plan's workspace (one block of device
+// memory, 256-byte aligned pieces).
+struct WorkspaceLayout {
+    size_t o_pjk = 0, o_ipk = 0, o_psiB = 0, o_psiA = 0, o_psiAS = 0, o_asum = 0;
+    size_t o_words = 0;  // finalize counter (+0), error word (+16), conservation (+32)
+    size_t o_nzr = 0, o_nzc = 0;
+    size_t bytes = 0;
+};
+constexpr size_t kWorkspaceWords = 64;
+
 struct PlanImpl {
     int device = 0;
     int dtype = BLDM_F64;
@@ -44,6 +54,8 @@ struct PlanImpl {
     // Workspace: one allocation carved into the pieces below.
     void* ws = nullptr;
     size_t ws_bytes = 0;
+    bool owns_ws = false;         // allocated by plan_setup (plan_free releases it)
+    WorkspaceLayout layout{};
     double* part_pjk = nullptr;   // [n_rr][y][z]
     double* part_ipk = nullptr;   // [n_bands][x][z]
     void* psiB = nullptr;         // [y][z]  T
@@ -52,6 +64,7 @@ struct PlanImpl {
     double* asum_part = nullptr;  // [n_ablk][z]
     unsigned* counter = nullptr;  // finalize last-block counter
     int* err = nullptr;           // device error word
+    unsigned long long* cons = nullptr;  // conservation residual (bits of a double >= 0)
     bool skip_zero = false;       // bldm_tuning::skip_zero_rows
     int* nz_rows = nullptr;       // [n_bands][x] rows with X != 0 per band (skip_zero)
     int* nz_cnt = nullptr;        // [n_bands][x + 1] running counts (skip_zero)
@@ -72,6 +85,9 @@ int plan_shard_step(PlanImpl* p, const void* dX, void* dS, const double* dalpha,
 int plan_shard_finish(PlanImpl* p, const double* dbeta, const double* d_red, int psi_mode,
                       cudaStream_t st);
 int plan_check(PlanImpl* p, cudaStream_t st);
+int plan_conservation_launch(PlanImpl* p, const void* dX, const void* dS, cudaStream_t st);
+int plan_setup_in(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, void* ws,
+                  size_t ws_cap, size_t* ws_needed, cudaStream_t st);
 
 int cuda_status(cudaError_t e);
 int lane_config(size_t z, size_t es, SweepCfg& c);

@@ -126,6 +126,27 @@ void* pick_sweep_f32_batch(int vec, int lpf, int mch, int mode, bool mr);
 // type per dtype) for bands of band_w columns.
 int launch_nz_rows(int dtype, const void* dX, long long x, long long y, int band_w, int n_bands,
                    int* nz_rows, int* nz_cnt, cudaStream_t st);
+// Row-sum conservation residual max_f |sum_k S(f,k) - X(f)| / max(X(f), 1)
+// over nf fibers of depth z, atomically maxed into *out (the bits of a
+// nonnegative double; clear it first).  A NaN sum yields a NaN residual.
+int launch_conservation(int dtype, const void* dX, const void* dS, long long nf, long long z,
+                        unsigned long long* out, cudaStream_t st);
+// The same over many instances in one launch: block b works on instance
+// i = max{i : block_off[i] <= b}.
+struct ConsInst {
+    const void* X;
+    const void* S;
+    long long nf, z;
+    unsigned long long* out;
+    int lpf, pad;
+};
+int launch_conservation_multi(int dtype, const ConsInst* d_insts, const int* d_block_off,
+                              int n_inst, int n_blocks, cudaStream_t st);
+int conservation_blocks(long long nf, long long z);
+ConsInst cons_inst(const void* X, const void* S, long long nf, long long z,
+                   unsigned long long* out);
+// The residual from the bits launch_conservation left.
+double cons_value(unsigned long long bits);
 int launch_init_S(int dtype, const void* dX, void* dS, long long nf, long long z, uint64_t seed,
                   cudaStream_t st);
 

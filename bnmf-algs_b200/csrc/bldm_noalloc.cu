@@ -25,11 +25,6 @@
 
 #include "bldm_internal.h"
 
-namespace bldm {
-int plan_setup_in(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, void* ws,
-                  size_t ws_cap, size_t* ws_needed, cudaStream_t st);
-}
-
 using namespace bldm;
 
 namespace {
@@ -45,7 +40,10 @@ std::mutex g_mu;
 void* g_scratch_dev_ptr[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device, looked up on the
-// first call on that device.
+// first call on that device and kept for the later ones.  A device reset (or
+// anything else that unloads this library's device code from the device)
+// invalidates the kept address; the public header tells callers not to use the
+// entry point on such a device again.
 int scratch_on_current_device(void** out) {
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);

@@ -65,6 +65,7 @@ struct Request {
     size_t iters = 0;
     double rel = 1.0;
     double log_marginal = 0.0;
+    double conservation = 0.0;
     // result in the storage type (fetch converts FP32 to FP64); left
     // uninitialised until the copy fills it (a zero fill of a GiB-sized result
     // would cost as much as the copy)
@@ -153,6 +154,7 @@ struct bldm_server {
     std::vector<int> free_slots;
     size_t retiring = 0;
     double* d_rel = nullptr;  // [max_active] by slot
+    unsigned long long* d_cons = nullptr;  // [2] conservation residual bits, by lane
     size_t used = 0, peak = 0, budget = 0;
     uint64_t next_id = 1;
     bldm_server_stats st{};
@@ -240,6 +242,16 @@ void bldm_server::retire_loop(int lane) {
                     status = lanes[lane].copy_out(r->Sf.get(), r->inst.S, n * 4);
                 }
             }
+            unsigned long long cons_bits = 0;
+            if (status == BLDM_OK)
+                status = cuda_status(cudaMemsetAsync(d_cons + lane, 0, 8, rstream));
+            if (status == BLDM_OK)
+                status = launch_conservation(cfg.dtype, r->inst.X, r->inst.S,
+                                             (long long)(r->x * r->y), (long long)r->z,
+                                             d_cons + lane, rstream);
+            if (status == BLDM_OK)
+                status = cuda_status(cudaMemcpyAsync(&cons_bits, d_cons + lane, 8,
+                                                     cudaMemcpyDeviceToHost, rstream));
             if (status == BLDM_OK)
                 status = bldm_log_marginal_S(r->inst.S, cfg.dtype, r->x, r->y, r->z,
                                              r->alpha.data(), r->beta.data(), r->a, r->b,
@@ -247,6 +259,7 @@ void bldm_server::retire_loop(int lane) {
             if (r->dmem) cudaFreeAsync(r->dmem, rstream);
             r->dmem = nullptr;
             if (status == BLDM_OK) status = cuda_status(cudaStreamSynchronize(rstream));
+            if (status == BLDM_OK) r->conservation = cons_value(cons_bits);
             {
                 std::lock_guard<std::mutex> lk(mu);
                 retiring -= 1;
@@ -450,8 +463,10 @@ int bldm_server_create(bldm_server** out, const bldm_server_config* cfg) {
         if (e == cudaSuccess) e = cudaEventCreate(&L.ev1);
     }
     if (e == cudaSuccess) e = cudaMalloc(&s->d_rel, cfg->max_active * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_cons, 2 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         if (s->d_rel) cudaFree(s->d_rel);
+        if (s->d_cons) cudaFree(s->d_cons);
         for (Lane& L : s->lanes) {
             if (L.ev0) cudaEventDestroy(L.ev0);
             if (L.ev1) cudaEventDestroy(L.ev1);
@@ -516,6 +531,7 @@ int bldm_server_destroy(bldm_server* s) {
         }
     }
     if (s->d_rel) cudaFree(s->d_rel);
+    if (s->d_cons) cudaFree(s->d_cons);
     delete s;
     return BLDM_OK;
 }
@@ -596,6 +612,7 @@ int bldm_server_fetch(bldm_server* s, uint64_t id, double* S_out, bldm_request_s
         rs->iterations = r->iters;
         rs->rel_change = r->rel;
         rs->log_marginal = r->log_marginal;
+        rs->conservation_residual = r->conservation;
         rs->status = r->status;
     }
     if (r->state == REQ_DONE && S_out) {

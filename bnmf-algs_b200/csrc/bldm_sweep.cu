@@ -394,9 +394,13 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
     return BLDM_OK;
 }
 
-int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_tuning* tune) {
+// Shape, launch configuration and workspace layout of a plan (no device
+// memory yet): plan_setup allocates the workspace, plan_setup_in places it in
+// memory the caller provides.  Both bind through plan_bind_workspace, so the
+// layout exists once.
+static int plan_configure(PlanImpl* p, size_t x, size_t y, size_t z, int dtype,
+                          const bldm_tuning* tune) {
     if (x == 0 || y == 0 || z == 0) return BLDM_ERR_BAD_ARG;
-    if (z > 1024) return BLDM_ERR_UNSUPPORTED;
     if (dtype != BLDM_F64 && dtype != BLDM_F32) return BLDM_ERR_BAD_ARG;
     BLDM_CU(cudaGetDevice(&p->device));
     p->dtype = dtype;
@@ -404,53 +408,57 @@ int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_
     p->y = y;
     p->z = z;
     p->esize = dtype == BLDM_F64 ? 8 : 4;
+    p->skip_zero = tune && tune->skip_zero_rows != 0;
     int rc = choose_cfg(p->cfg, x, y, z, p->esize, num_sms_of(p->device), tune);
     if (rc) return rc;
     const SweepCfg& c = p->cfg;
+    WorkspaceLayout& L = p->layout;
     const size_t a = 256;
     size_t off = 0;
-    const size_t o_pjk = off;
+    L.o_pjk = off;
     off = align_up(off + size_t(c.n_rr) * y * z * 8, a);
-    const size_t o_ipk = off;
+    L.o_ipk = off;
     off = align_up(off + size_t(c.n_bands) * x * z * 8, a);
-    const size_t o_psiB = off;
+    L.o_psiB = off;
     off = align_up(off + y * z * p->esize, a);
-    const size_t o_psiA = off;
+    L.o_psiA = off;
     off = align_up(off + x * z * p->esize, a);
-    const size_t o_psiAS = off;
+    L.o_psiAS = off;
     off = align_up(off + z * p->esize, a);
-    const size_t o_asum = off;
+    L.o_asum = off;
     off = align_up(off + size_t(c.n_ablk) * z * 8, a);
-    const size_t o_cnt = off;
-    off = align_up(off + 64, a);
-    p->skip_zero = tune && tune->skip_zero_rows != 0;
-    const size_t o_nzr = off;
+    L.o_words = off;  // finalize counter | error word | conservation residual
+    off = align_up(off + kWorkspaceWords, a);
+    L.o_nzr = off;
     if (p->skip_zero) off = align_up(off + size_t(c.n_bands) * x * 4, a);
-    const size_t o_nzc = off;
+    L.o_nzc = off;
     if (p->skip_zero) off = align_up(off + size_t(c.n_bands) * (x + 1) * 4, a);
-    p->ws_bytes = off;
-    cudaError_t e = cudaMalloc(&p->ws, p->ws_bytes);
-    if (e != cudaSuccess) {
-        p->ws = nullptr;
-        return cuda_status(e);
-    }
-    char* base = static_cast<char*>(p->ws);
-    p->part_pjk = reinterpret_cast<double*>(base + o_pjk);
-    p->part_ipk = reinterpret_cast<double*>(base + o_ipk);
-    p->psiB = base + o_psiB;
-    p->psiA = base + o_psiA;
-    p->psiAS = base + o_psiAS;
-    p->asum_part = reinterpret_cast<double*>(base + o_asum);
-    p->counter = reinterpret_cast<unsigned*>(base + o_cnt);
-    p->err = reinterpret_cast<int*>(base + o_cnt + 16);
-    p->nz_rows = p->skip_zero ? reinterpret_cast<int*>(base + o_nzr) : nullptr;
-    p->nz_cnt = p->skip_zero ? reinterpret_cast<int*>(base + o_nzc) : nullptr;
-    BLDM_CU(cudaMemset(base + o_cnt, 0, 64));
-    // Opt the selected kernels into large dynamic shared memory.
+    L.bytes = off;
+    return BLDM_OK;
+}
+
+// Points the plan's pieces into `ws` (at least p->layout.bytes bytes) and opts
+// the plan's kernels into their dynamic shared memory.
+static int plan_bind_workspace(PlanImpl* p, void* ws) {
+    const WorkspaceLayout& L = p->layout;
+    p->ws_bytes = L.bytes;
+    char* base = static_cast<char*>(ws);
+    p->part_pjk = reinterpret_cast<double*>(base + L.o_pjk);
+    p->part_ipk = reinterpret_cast<double*>(base + L.o_ipk);
+    p->psiB = base + L.o_psiB;
+    p->psiA = base + L.o_psiA;
+    p->psiAS = base + L.o_psiAS;
+    p->asum_part = reinterpret_cast<double*>(base + L.o_asum);
+    p->counter = reinterpret_cast<unsigned*>(base + L.o_words);
+    p->err = reinterpret_cast<int*>(base + L.o_words + 16);
+    p->cons = reinterpret_cast<unsigned long long*>(base + L.o_words + 32);
+    p->nz_rows = p->skip_zero ? reinterpret_cast<int*>(base + L.o_nzr) : nullptr;
+    p->nz_cnt = p->skip_zero ? reinterpret_cast<int*>(base + L.o_nzc) : nullptr;
+    const SweepCfg& c = p->cfg;
     for (int mode = SWEEP_SUMS; mode <= SWEEP_COMPACT; ++mode)
         for (int ap = 0; ap < 2; ++ap) {
             void* fn = nullptr;
-            if (dtype == BLDM_F64)
+            if (p->dtype == BLDM_F64)
                 fn = reinterpret_cast<void*>(pick_sweep<double>(c, mode, ap != 0));
             else
                 fn = reinterpret_cast<void*>(pick_sweep<float>(c, mode, ap != 0));
@@ -458,6 +466,21 @@ int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_
             const int rc_attr = ensure_smem_attr(fn, c.smem_update);
             if (rc_attr) return rc_attr;
         }
+    return BLDM_OK;
+}
+
+int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_tuning* tune) {
+    int rc = plan_configure(p, x, y, z, dtype, tune);
+    if (rc) return rc;
+    cudaError_t e = cudaMalloc(&p->ws, p->layout.bytes);
+    if (e != cudaSuccess) {
+        p->ws = nullptr;
+        return cuda_status(e);
+    }
+    p->owns_ws = true;
+    rc = plan_bind_workspace(p, p->ws);
+    if (rc) return rc;
+    BLDM_CU(cudaMemset(static_cast<char*>(p->ws) + p->layout.o_words, 0, kWorkspaceWords));
     return BLDM_OK;
 }
 
@@ -467,64 +490,21 @@ int plan_setup(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, const bldm_
 // error word are cleared on `st`.
 int plan_setup_in(PlanImpl* p, size_t x, size_t y, size_t z, int dtype, void* ws,
                   size_t ws_cap, size_t* ws_needed, cudaStream_t st) {
-    if (x == 0 || y == 0 || z == 0 || !ws) return BLDM_ERR_BAD_ARG;
-    if (z > 1024) return BLDM_ERR_UNSUPPORTED;
-    if (dtype != BLDM_F64 && dtype != BLDM_F32) return BLDM_ERR_BAD_ARG;
-    BLDM_CU(cudaGetDevice(&p->device));
-    p->dtype = dtype;
-    p->x = x;
-    p->y = y;
-    p->z = z;
-    p->esize = dtype == BLDM_F64 ? 8 : 4;
-    int rc = choose_cfg(p->cfg, x, y, z, p->esize, num_sms_of(p->device), nullptr);
+    if (!ws) return BLDM_ERR_BAD_ARG;
+    int rc = plan_configure(p, x, y, z, dtype, nullptr);
     if (rc) return rc;
-    const SweepCfg& c = p->cfg;
-    const size_t a = 256;
-    size_t off = 0;
-    const size_t o_pjk = off;
-    off = align_up(off + size_t(c.n_rr) * y * z * 8, a);
-    const size_t o_ipk = off;
-    off = align_up(off + size_t(c.n_bands) * x * z * 8, a);
-    const size_t o_psiB = off;
-    off = align_up(off + y * z * p->esize, a);
-    const size_t o_psiA = off;
-    off = align_up(off + x * z * p->esize, a);
-    const size_t o_psiAS = off;
-    off = align_up(off + z * p->esize, a);
-    const size_t o_asum = off;
-    off = align_up(off + size_t(c.n_ablk) * z * 8, a);
-    const size_t o_cnt = off;
-    off = align_up(off + 64, a);
-    if (ws_needed) *ws_needed = off;
-    if (off > ws_cap) return BLDM_ERR_TOO_LARGE;
-    p->ws = ws;  // not owned: never pass this plan to plan_free
-    p->ws_bytes = off;
-    char* base = static_cast<char*>(ws);
-    p->part_pjk = reinterpret_cast<double*>(base + o_pjk);
-    p->part_ipk = reinterpret_cast<double*>(base + o_ipk);
-    p->psiB = base + o_psiB;
-    p->psiA = base + o_psiA;
-    p->psiAS = base + o_psiAS;
-    p->asum_part = reinterpret_cast<double*>(base + o_asum);
-    p->counter = reinterpret_cast<unsigned*>(base + o_cnt);
-    p->err = reinterpret_cast<int*>(base + o_cnt + 16);
-    BLDM_CU(cudaMemsetAsync(base + o_cnt, 0, 64, st));
-    for (int mode = SWEEP_SUMS; mode <= SWEEP_COMPACT; ++mode)
-        for (int ap = 0; ap < 2; ++ap) {
-            void* fn = nullptr;
-            if (dtype == BLDM_F64)
-                fn = reinterpret_cast<void*>(pick_sweep<double>(c, mode, ap != 0));
-            else
-                fn = reinterpret_cast<void*>(pick_sweep<float>(c, mode, ap != 0));
-            if (!fn) return BLDM_ERR_UNSUPPORTED;
-            const int rc_attr = ensure_smem_attr(fn, c.smem_update);
-            if (rc_attr) return rc_attr;
-        }
+    if (ws_needed) *ws_needed = p->layout.bytes;
+    if (p->layout.bytes > ws_cap) return BLDM_ERR_TOO_LARGE;
+    p->ws = ws;  // not owned: plan_free leaves it alone
+    p->owns_ws = false;
+    rc = plan_bind_workspace(p, ws);
+    if (rc) return rc;
+    BLDM_CU(cudaMemsetAsync(static_cast<char*>(ws) + p->layout.o_words, 0, kWorkspaceWords, st));
     return BLDM_OK;
 }
 
 void plan_free(PlanImpl* p) {
-    if (p->ws) cudaFree(p->ws);
+    if (p->ws && p->owns_ws) cudaFree(p->ws);
     p->ws = nullptr;
 }
 
@@ -818,15 +798,31 @@ int launch_init_S(int dtype, const void* dX, void* dS, long long nf, long long z
     return cuda_status(cudaGetLastError());
 }
 
+// Reads the error word behind the work queued on `st` and clears it, all in
+// the order of `st` (no legacy-stream copy that would wait for the device's
+// other blocking streams).
 int plan_check(PlanImpl* p, cudaStream_t st) {
-    BLDM_CU(cudaStreamSynchronize(st));
     int herr = 0;
-    BLDM_CU(cudaMemcpy(&herr, p->err, sizeof(int), cudaMemcpyDeviceToHost));
+    BLDM_CU(cudaMemcpyAsync(&herr, p->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BLDM_CU(cudaStreamSynchronize(st));
     if (herr != 0) {
-        BLDM_CU(cudaMemset(p->err, 0, sizeof(int)));
+        BLDM_CU(cudaMemsetAsync(p->err, 0, sizeof(int), st));
+        BLDM_CU(cudaStreamSynchronize(st));
         return BLDM_ERR_TIMEOUT;
     }
     return BLDM_OK;
+}
+
+// Row-sum conservation residual of (X, S): max over fibers of
+// |sum_k S(i,j,k) - X(i,j)| / max(X(i,j), 1), in FP64.  Enqueued on `st`; the
+// value lands in p->cons (the bits of a nonnegative double).
+int plan_conservation_launch(PlanImpl* p, const void* dX, const void* dS, cudaStream_t st) {
+    if (!p || !p->ws || !dX || !dS) return BLDM_ERR_BAD_ARG;
+    BLDM_CU(cudaMemsetAsync(p->cons, 0, sizeof(unsigned long long), st));
+    const int rc = launch_conservation(p->dtype, dX, dS, (long long)(p->x * p->y),
+                                       (long long)p->z, p->cons, st);
+    p->launches += 1;
+    return rc;
 }
 
 }  // namespace bldm

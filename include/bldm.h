@@ -85,6 +85,13 @@ typedef struct bldm_stats {
     uint64_t iterations;    /* iterations run */
     uint64_t kernel_launches; /* kernels launched by the call */
     double rel_change;      /* ||S_last - S_prev||_1 / ||S_last||_1 (batch/server) */
+    /* Row-sum conservation of the result, max_ij |sum_k S(i,j,k) - X(i,j)| /
+     * max(X(i,j), 1), computed on the device after the last iteration.  The
+     * reference's tests check S_ij+ against X after a solve
+     * (test/bld/bld_mult/test_bld_mult.cpp:67-71,80-84); the update uses the
+     * pre-update sums (bld_mult_funcs.hpp:307-327), so it is zero only at the
+     * fixed point and is reported rather than enforced. */
+    double conservation_residual;
 } bldm_stats;
 
 /* ------------------------------------------------------------------------
@@ -169,10 +176,13 @@ int bldm_plan_run(bldm_plan* plan, const void* d_X, const double* d_alpha,
  * shapes whose scratch exceeds it return BLDM_ERR_TOO_LARGE (1024x1024x64 FP64
  * needs 22.5 MB).  The caller passes device buffers as for bldm_plan_run (dtype
  * is BLDM_F64 or BLDM_F32).  The first call on a device looks up the array's
- * device address on that device (make that first call before any stream
- * capture).  All calls on a device share the array, and calls that overlap on
- * the GPU race.  Synchronises `stream` before returning and reports a
- * device-side error as BLDM_ERR_TIMEOUT. */
+ * device address on that device and keeps it for later calls (make that first
+ * call before any stream capture); after cudaDeviceReset, or anything else
+ * that unloads the library's device code from that device, the kept address no
+ * longer belongs to the new context, so do not call this entry point on that
+ * device again in the same process.  All calls on a device share the array,
+ * and calls that overlap on the GPU race.  Synchronises `stream` before
+ * returning and reports a device-side error as BLDM_ERR_TIMEOUT. */
 int bldm_solve_device_noalloc(const void* d_X, const double* d_alpha,
                               const double* d_beta, void* d_S, size_t x, size_t y,
                               size_t z, int dtype, size_t max_iter, int psi_mode,
@@ -180,6 +190,13 @@ int bldm_solve_device_noalloc(const void* d_X, const double* d_alpha,
 /* Synchronises `stream` and reports a device-side error recorded by the
  * plan's kernels (BLDM_ERR_TIMEOUT) or a CUDA error. */
 int bldm_plan_check(bldm_plan* plan, void* stream);
+/* Row-sum conservation residual max_ij |sum_k S(i,j,k) - X(i,j)| / max(X(i,j), 1)
+ * of device buffers of the plan's shape and dtype, computed on the device (one
+ * read of S, FP64 sums) behind the work queued on `stream`; synchronises
+ * `stream`.  The check the reference's tests make after a solve
+ * (test/bld/bld_mult/test_bld_mult.cpp:67-71,80-84). */
+int bldm_plan_conservation(bldm_plan* plan, const void* d_X, const void* d_S, void* stream,
+                           double* residual);
 /* Draw the seeded initial S on the device (see bldm_solve_f64). */
 int bldm_plan_init_S(bldm_plan* plan, const void* d_X, void* d_S, uint64_t seed,
                      void* stream);
@@ -332,6 +349,10 @@ int bldm_batch_check(bldm_batch* batch, void* stream);
 /* Instance idx's S (x*y*z) and the relative change sum|S_n - S_{n-1}| /
  * sum|S_n| of the run's last iteration; either output may be NULL. */
 int bldm_batch_get(bldm_batch* batch, size_t idx, double* S_out, double* rel_change);
+/* Row-sum conservation residual (as bldm_plan_conservation) of every
+ * instance's current S, residuals[n], in one device launch behind `stream`;
+ * synchronises `stream`. */
+int bldm_batch_conservation(bldm_batch* batch, double* residuals, void* stream);
 /* Device buffers of instance idx (storage dtype), for device-resident callers. */
 int bldm_batch_device_ptrs(bldm_batch* batch, size_t idx, void** d_X, void** d_S);
 int bldm_batch_info(const bldm_batch* batch, size_t* n_classes, size_t* device_bytes,
@@ -405,6 +426,7 @@ typedef struct bldm_request_stats {
     double rel_change;       /* relative change of S at retirement */
     double log_marginal;     /* log_marginal_S of the result (FP64) */
     int status;              /* bldm_status of the request */
+    double conservation_residual; /* as bldm_stats, computed at retirement */
 } bldm_request_stats;
 typedef struct bldm_server_stats {
     uint64_t submitted, completed, failed, rounds, iterations;

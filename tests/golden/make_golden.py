@@ -1,9 +1,9 @@
 """Generates the committed golden fixtures under tests/golden/.
 
-Run in a container that has the reference checkout (read-only) at
-/root/reference:
+Run where a checkout of the reference (eozd/bnmf-algs) is available, giving
+its root directory:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <path to the reference checkout>
 
 Fixtures:
   kat_8x10.json   the 8x10 count matrix of the reference's known-answer test
@@ -52,7 +52,8 @@ def parse_kat_matrix(reference):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="root directory of a checkout of the reference (eozd/bnmf-algs)")
     args = ap.parse_args()
     import oracle as O
     import mpmath

@@ -235,3 +235,62 @@ def test_batch_zero_rows_from_dirty_S0(bldm, oracle, workloads):
         ref = np.abs(s10 - s9).sum() / np.abs(s10).sum()
         assert abs(rel - ref) <= 1e-9 * ref + 1e-15
     b.close()
+
+
+@pytest.fixture(scope="module")
+def benchmarked_batch(workloads, oracle):
+    """The 512-instance uneven batch the benchmark runs (x, y log-uniform in
+    [32, 512], z in {4, 8, 16, 32, 64}, 150 iterations), with a seeded sample
+    of 16 instances whose initial S is the oracle's and whose 150-iteration
+    oracle solutions (FP64, psi_appr) are computed once here."""
+    shapes = workloads.batch_shapes(512, 3)
+    probs = [workloads.batch_instance(s, 1000 + 3 * 100003 + k) for k, s in enumerate(shapes)]
+    sample = sorted(np.random.default_rng(2024).choice(len(shapes), 16, replace=False).tolist())
+    oracle.set_threads(0)
+    ref = {}
+    for k in sample:
+        pr = probs[k]
+        S0 = oracle.init_S(pr["X"], pr["z"], k)
+        S = oracle.bld_mult(pr["X"], pr["z"], pr["alpha"], pr["beta"], 150, oracle.PSI_APPR,
+                            1e-50, S0=S0)
+        ref[k] = (S0, S, oracle.log_marginal_S(S, pr["alpha"], pr["beta"], pr["a"], pr["b"]))
+    return shapes, probs, sample, ref
+
+
+def _run_benchmarked(bldm, shapes, probs, ref, dtype):
+    import torch
+    b = bldm.Batch(shapes, dtype=dtype)
+    for k, pr in enumerate(probs):
+        S0 = ref[k][0] if k in ref else None
+        b.set(k, pr["X"], pr["alpha"], pr["beta"], S0, seed=k)
+    stream = torch.cuda.Stream()
+    b.autotune(probe_iters=3, stream=stream)
+    b.run(150, bldm.PSI_APPR, 1e-50, True, stream)
+    b.check(stream)
+    return b
+
+
+def test_benchmarked_batch_sample_fp64_matches_oracle(bldm, oracle, benchmarked_batch):
+    shapes, probs, sample, ref = benchmarked_batch
+    b = _run_benchmarked(bldm, shapes, probs, ref, bldm.F64)
+    cons = b.conservation()
+    for k in sample:
+        S, _ = b.get(k)
+        assert rel_err(S, ref[k][1]) <= 1e-9, (k, shapes[k], rel_err(S, ref[k][1]))
+        X = probs[k]["X"]
+        want = float((np.abs(S.sum(axis=2) - X) / np.maximum(X, 1.0)).max())
+        assert abs(cons[k] - want) <= 1e-12 * max(want, 1.0)
+    b.close()
+
+
+def test_benchmarked_batch_sample_fp32_log_marginal(bldm, oracle, benchmarked_batch):
+    shapes, probs, sample, ref = benchmarked_batch
+    b = _run_benchmarked(bldm, shapes, probs, ref, bldm.F32)
+    for k in sample:
+        pr = probs[k]
+        S, _ = b.get(k)
+        assert np.all(np.isfinite(S))
+        lm = oracle.log_marginal_S(S.astype(np.float32), pr["alpha"], pr["beta"], pr["a"],
+                                   pr["b"])
+        assert abs(lm - ref[k][2]) <= 1e-5 * abs(ref[k][2]), (k, shapes[k], lm, ref[k][2])
+    b.close()

@@ -95,6 +95,9 @@ def test_server_fp64_matches_oracle_and_stops(bldm, workloads, oracle):
     assert np.abs(S - ref).max() / np.abs(ref).max() <= 1e-9
     lm = oracle.log_marginal_S(S, p.alpha, p.beta, p.a, p.b)
     assert abs(st["log_marginal"] - lm) <= 1e-10 * abs(lm)
+    # row-sum conservation residual computed on the device at retirement
+    cons = float((np.abs(S.sum(axis=2) - X) / np.maximum(X, 1.0)).max())
+    assert abs(st["conservation_residual"] - cons) <= 1e-12 * max(cons, 1.0)
     srv.close()
 
 

@@ -62,11 +62,24 @@ def test_noalloc_matches_plan_api_twice(bldm, workloads, oracle, dtype, tol):
         assert _rel(got, ref) <= tol, (call, _rel(got, ref))
 
 
-def test_noalloc_rejects_shapes_beyond_its_scratch(bldm):
-    # 4096 x 4096 x 64 in FP64 needs far more than the fixed 32 MiB scratch;
-    # the size check happens before any device work touches the buffers.
+@pytest.mark.parametrize("dtype", [0, 1])
+def test_noalloc_rejects_shapes_beyond_its_scratch(bldm, dtype):
+    # 4096 x 4096 x 64 needs far more than the fixed 32 MiB scratch in either
+    # storage type; the size check happens before any device work touches the
+    # buffers.
     d = torch.zeros(16, dtype=torch.float64, device="cuda")
     p = ctypes.c_void_p(d.data_ptr())
-    rc = bldm.lib().bldm_solve_device_noalloc(p, p, p, p, 4096, 4096, 64, bldm.F64, 5,
+    rc = bldm.lib().bldm_solve_device_noalloc(p, p, p, p, 4096, 4096, 64, dtype, 5,
                                               bldm.PSI_APPR, 1e-50, None)
     assert rc == bldm.ERR_TOO_LARGE
+
+
+def test_noalloc_accepts_the_documented_fit(bldm):
+    # 1024 x 1024 x 64 in FP64 needs 22.5 MB of scratch and fits.  With
+    # max_iter = 0 the call sets up its scratch and returns without touching
+    # the (deliberately small) buffers.
+    d = torch.zeros(16, dtype=torch.float64, device="cuda")
+    p = ctypes.c_void_p(d.data_ptr())
+    rc = bldm.lib().bldm_solve_device_noalloc(p, p, p, p, 1024, 1024, 64, bldm.F64, 0,
+                                              bldm.PSI_APPR, 1e-50, None)
+    assert rc == bldm.OK
