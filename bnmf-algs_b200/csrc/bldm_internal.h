@@ -33,6 +33,11 @@ struct SweepCfg {
     size_t smem_update, smem_sums;
     int n_ablk, rows_per_ablk;  // finalize: row blocks for alpha_eph
     int fin_threads;
+    // Long fibers (z beyond the lane layout): the two-pass kernels of
+    // bldm_long.cu over n_kc k-chunks x n_bands bands of kLongBand columns x
+    // n_rr row ranges; vec/lpf/mch/stages are unused.
+    bool long_mode = false;
+    int n_kc = 0;
 };
 
 // Byte offsets of the pieces of a plan's workspace (one block of device
@@ -41,6 +46,7 @@ struct WorkspaceLayout {
     size_t o_pjk = 0, o_ipk = 0, o_psiB = 0, o_psiA = 0, o_psiAS = 0, o_asum = 0;
     size_t o_words = 0;  // finalize counter (+0), error word (+16), conservation (+32)
     size_t o_nzr = 0, o_nzc = 0;
+    size_t o_fsum = 0;   // long fibers: per-fiber sums [x*y] double4
     size_t bytes = 0;
 };
 constexpr size_t kWorkspaceWords = 64;
@@ -68,6 +74,7 @@ struct PlanImpl {
     bool skip_zero = false;       // bldm_tuning::skip_zero_rows
     int* nz_rows = nullptr;       // [n_bands][x] rows with X != 0 per band (skip_zero)
     int* nz_cnt = nullptr;        // [n_bands][x + 1] running counts (skip_zero)
+    void* fsum = nullptr;         // [x*y] double4 fiber sums (long fibers)
     uint64_t launches = 0;
 };
 

@@ -110,6 +110,29 @@ template <typename T> struct BatchFinParams {
     int plus_appr, minus_appr;
 };
 
+// Long fibers (depths beyond the fused sweep's lane layout; bldm_long.cu):
+// tiles of (k-chunk of kLongThreads, band of kLongBand columns, row range).
+constexpr int kLongThreads = 256;
+constexpr int kLongBand = 8;
+template <typename T> struct LongSweepParams {
+    T* S;
+    const T* X;
+    const T* psiB;       // psi(beta_eph) [y][z]
+    const T* psiA;       // psi(alpha_eph) [x][z]
+    const T* psiAS;      // psi(sum_i alpha_eph) [z]
+    double* part_pjk;    // [n_rr][y][z]
+    double* part_ipk;    // [n_bands][x][z]
+    double4* fsum;       // [x*y] (S_ij+, an, ad, -) of the fiber before the update
+    long long x, y, z;
+    int n_kc, n_bands, n_rr, rr_base, rr_extra;
+    double eps;
+};
+// update: the fiber sums pass and the update pass (2 launches); otherwise the
+// axis sums of S alone (1 launch).  params points to LongSweepParams<T> of the
+// dtype.  pdl: launch with programmatic stream serialisation.
+int launch_long_sweep(int dtype, const void* params, bool update, bool appr, bool pdl,
+                      cudaStream_t st, uint64_t* launches);
+
 // Kernel entry points by lane shape (defined in bldm_sweep.cu).  mode: 0 the
 // axis sums of S, 1 the update, 2 the compact update (rows listed in
 // SweepInst::nz_rows only, no stores of zeros: valid once an update has

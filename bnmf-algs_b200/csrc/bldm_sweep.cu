@@ -76,7 +76,7 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
         }
         return;
     }
-    __shared__ double acc[1024];
+    __shared__ double acc[2 * kFinThreads];
     __shared__ unsigned last;
     const int b = blk - p.nbB;
     const long long i0 = (long long)b * p.rows_per_ablk;
@@ -84,6 +84,9 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
     const int KT = (int)min(z, (long long)kFinThreads);
     const int R = kFinThreads / KT;
     const int sub = tid / KT;
+    // R > 1 (z < 256): R row groups of KT threads, combined through acc
+    // (R * z <= 2 * kFinThreads entries); R == 1: a thread's sum over the
+    // block's rows is the block's partial itself (any z)
     if (sub < R) {
         for (long long k = tid % KT; k < z; k += KT) {
             double a = 0.0;
@@ -93,14 +96,19 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
                 p.psiA[i * z + k] = T(psi_mode_f64(ae, minus_appr != 0));
                 a += ae;
             }
-            acc[sub * z + k] = a;
+            if (R == 1)
+                p.asum_part[(long long)b * z + k] = a;
+            else
+                acc[sub * z + k] = a;
         }
     }
-    __syncthreads();
-    for (long long k = tid; k < z; k += kFinThreads) {
-        double a = 0.0;
-        for (int r = 0; r < R; ++r) a += acc[r * z + k];
-        p.asum_part[(long long)b * z + k] = a;
+    if (R > 1) {
+        __syncthreads();
+        for (long long k = tid; k < z; k += kFinThreads) {
+            double a = 0.0;
+            for (int r = 0; r < R; ++r) a += acc[r * z + k];
+            p.asum_part[(long long)b * z + k] = a;
+        }
     }
     __threadfence();
     __syncthreads();
@@ -109,21 +117,31 @@ __device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int
     if (last) {
         __threadfence();
         // group r < R sums blocks r, r + R, r + 2R, ... of column k
-        if (sub < R) {
-            for (long long k = tid % KT; k < z; k += KT) {
-                const int nb = (p.n_ablk - sub + R - 1) / R;
-                acc[sub * z + k] =
-                    sum_strided<true, W>(p.asum_part + (long long)sub * z + k, (long long)R * z, nb);
+        if (R == 1) {
+            for (long long k = tid; k < z; k += kFinThreads) {
+                const double a = sum_strided<true, W>(p.asum_part + k, z, p.n_ablk);
+                if (p.red)
+                    p.red[p.y * z + k] = a;
+                else
+                    p.psiAS[k] = T(psi_mode_f64(a, minus_appr != 0));
             }
-        }
-        __syncthreads();
-        for (long long k = tid; k < z; k += kFinThreads) {
-            double a = 0.0;
-            for (int r = 0; r < R; ++r) a += acc[r * z + k];
-            if (p.red)
-                p.red[p.y * z + k] = a;
-            else
-                p.psiAS[k] = T(psi_mode_f64(a, minus_appr != 0));
+        } else {
+            if (sub < R) {
+                for (long long k = tid % KT; k < z; k += KT) {
+                    const int nb = (p.n_ablk - sub + R - 1) / R;
+                    acc[sub * z + k] = sum_strided<true, W>(p.asum_part + (long long)sub * z + k,
+                                                            (long long)R * z, nb);
+                }
+            }
+            __syncthreads();
+            for (long long k = tid; k < z; k += kFinThreads) {
+                double a = 0.0;
+                for (int r = 0; r < R; ++r) a += acc[r * z + k];
+                if (p.red)
+                    p.red[p.y * z + k] = a;
+                else
+                    p.psiAS[k] = T(psi_mode_f64(a, minus_appr != 0));
+            }
         }
         if (p.delta_part && tid < 32) {
             // lanes take tiles t = lane, lane + 32, ...; then a fixed-order tree
@@ -321,9 +339,51 @@ int lane_config(size_t z, size_t es, SweepCfg& c) {
     return BLDM_OK;
 }
 
+// Finalize row blocks: one row per thread (R rows of KT columns per block) up
+// to ~256 blocks, so that a thread's sums of the band partials are not
+// serialised over several rows.
+static void finalize_blocks(SweepCfg& c, size_t x, size_t z) {
+    const int KT = int(std::min<size_t>(z, kFinThreads));
+    const int R = kFinThreads / KT;
+    long rows = std::max<long>(R, long((x + 255) / 256));
+    c.rows_per_ablk = int(rows);
+    c.n_ablk = int((x + rows - 1) / rows);
+    c.fin_threads = kFinThreads;
+}
+
+// Long fibers: tiles of (k-chunk, band of kLongBand columns, row range) for the
+// two-pass kernels.  At least 32 rows per tile where x allows (each tile writes
+// one S_+jk partial row per column, 1/rows of the S it sweeps) and about four
+// waves of eight resident tiles per SM.
+static int choose_long_cfg(SweepCfg& c, size_t x, size_t y, size_t z, int num_sms,
+                           const bldm_tuning* tune) {
+    if (tune && (tune->stages > 0 || tune->ctas_per_sm > 0)) return BLDM_ERR_UNSUPPORTED;
+    c = SweepCfg{};
+    c.long_mode = true;
+    c.vec = 1;
+    c.lpf = 32;
+    c.warps = kSweepWarps;
+    c.wpr = kSweepWarps;
+    c.band_w = kLongBand;
+    c.n_bands = int((y + kLongBand - 1) / kLongBand);
+    c.n_kc = int((z + kLongThreads - 1) / kLongThreads);
+    const long per_rr = long(c.n_kc) * c.n_bands;
+    const long target = long(num_sms) * 8 * 4;
+    long nrr = (target + per_rr - 1) / per_rr;
+    nrr = std::min(nrr, std::max(1L, long(x / 32)));
+    if (tune && tune->row_ranges > 0) nrr = tune->row_ranges;
+    nrr = std::max(1L, std::min(long(x), nrr));
+    c.n_rr = int(nrr);
+    c.rr_base = int(x / nrr);
+    c.rr_extra = int(x % nrr);
+    finalize_blocks(c, x, z);
+    return BLDM_OK;
+}
+
 static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int num_sms,
                       const bldm_tuning* tune) {
-    if (lane_config(z, es, c) != BLDM_OK) return BLDM_ERR_UNSUPPORTED;
+    if (lane_config(z, es, c) != BLDM_OK) return choose_long_cfg(c, x, y, z, num_sms, tune);
+    c.long_mode = false;
     c.warps = kSweepWarps;
     const int fpw = 32 / c.lpf;
     // warps per row: as few as cover y, so that narrow rows share a stage
@@ -382,15 +442,7 @@ static int choose_cfg(SweepCfg& c, size_t x, size_t y, size_t z, size_t es, int 
     c.n_rr = int(nrr);
     c.rr_base = int(x / nrr);
     c.rr_extra = int(x % nrr);
-    // finalize row blocks: one row per thread (R rows of KT columns per block)
-    // up to ~256 blocks, so that a thread's sums of the band partials are not
-    // serialised over several rows
-    const int KT = int(std::min<size_t>(z, kFinThreads));
-    const int R = kFinThreads / KT;
-    long rows = std::max<long>(R, long((x + 255) / 256));
-    c.rows_per_ablk = int(rows);
-    c.n_ablk = int((x + rows - 1) / rows);
-    c.fin_threads = kFinThreads;
+    finalize_blocks(c, x, z);
     return BLDM_OK;
 }
 
@@ -412,6 +464,8 @@ static int plan_configure(PlanImpl* p, size_t x, size_t y, size_t z, int dtype,
     int rc = choose_cfg(p->cfg, x, y, z, p->esize, num_sms_of(p->device), tune);
     if (rc) return rc;
     const SweepCfg& c = p->cfg;
+    // the long-fiber kernels sweep every row (no row lists)
+    if (c.long_mode) p->skip_zero = false;
     WorkspaceLayout& L = p->layout;
     const size_t a = 256;
     size_t off = 0;
@@ -433,6 +487,8 @@ static int plan_configure(PlanImpl* p, size_t x, size_t y, size_t z, int dtype,
     if (p->skip_zero) off = align_up(off + size_t(c.n_bands) * x * 4, a);
     L.o_nzc = off;
     if (p->skip_zero) off = align_up(off + size_t(c.n_bands) * (x + 1) * 4, a);
+    L.o_fsum = off;
+    if (c.long_mode) off = align_up(off + x * y * sizeof(double4), a);
     L.bytes = off;
     return BLDM_OK;
 }
@@ -455,6 +511,8 @@ static int plan_bind_workspace(PlanImpl* p, void* ws) {
     p->nz_rows = p->skip_zero ? reinterpret_cast<int*>(base + L.o_nzr) : nullptr;
     p->nz_cnt = p->skip_zero ? reinterpret_cast<int*>(base + L.o_nzc) : nullptr;
     const SweepCfg& c = p->cfg;
+    p->fsum = c.long_mode ? base + L.o_fsum : nullptr;
+    if (c.long_mode) return BLDM_OK;  // no dynamic shared memory
     for (int mode = SWEEP_SUMS; mode <= SWEEP_COMPACT; ++mode)
         for (int ap = 0; ap < 2; ++ap) {
             void* fn = nullptr;
@@ -572,9 +630,74 @@ static FinParams<T> fin_params(PlanImpl* p, const double* dalpha, const double* 
 }
 
 template <typename T>
+static LongSweepParams<T> long_params(PlanImpl* p, const void* dX, void* dS, double eps) {
+    const SweepCfg& c = p->cfg;
+    LongSweepParams<T> l;
+    l.S = static_cast<T*>(dS);
+    l.X = static_cast<const T*>(dX);
+    l.psiB = static_cast<const T*>(p->psiB);
+    l.psiA = static_cast<const T*>(p->psiA);
+    l.psiAS = static_cast<const T*>(p->psiAS);
+    l.part_pjk = p->part_pjk;
+    l.part_ipk = p->part_ipk;
+    l.fsum = static_cast<double4*>(p->fsum);
+    l.x = (long long)p->x;
+    l.y = (long long)p->y;
+    l.z = (long long)p->z;
+    l.n_kc = c.n_kc;
+    l.n_bands = c.n_bands;
+    l.n_rr = c.n_rr;
+    l.rr_base = c.rr_base;
+    l.rr_extra = c.rr_extra;
+    l.eps = eps;
+    return l;
+}
+
+// The iterations of a long-fiber plan: sums of S0, finalize, then per iteration
+// the fiber-sums pass, the update pass and the finalize.  Events (profiling)
+// bracket the two passes of each update.
+template <typename T>
+static int run_long(PlanImpl* p, const void* dX, const double* dalpha, const double* dbeta,
+                    void* dS, size_t max_iter, int psi_mode, double eps, cudaStream_t st,
+                    cudaEvent_t* ev, size_t nev) {
+    const int plus_appr = psi_mode != BLDM_PSI_EXACT;
+    const int minus_appr = psi_mode == BLDM_PSI_APPR;
+    const LongSweepParams<T> lp = long_params<T>(p, dX, dS, eps);
+    const FinParams<T> fp = fin_params<T>(p, dalpha, dbeta, plus_appr, minus_appr);
+    const dim3 grid_f(unsigned(fp.f.nbB + fp.f.n_ablk));
+    const int dt = sizeof(T) == 8 ? BLDM_F64 : BLDM_F32;
+    const bool pdl = ev == nullptr;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    auto finalize = [&]() {
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = grid_f;
+        lc.blockDim = dim3(kFinThreads);
+        lc.stream = st;
+        lc.attrs = pdl ? attr : nullptr;
+        lc.numAttrs = pdl ? 1 : 0;
+        p->launches += 1;
+        return cuda_status(cudaLaunchKernelEx(&lc, finalize_kernel<T>, fp));
+    };
+    int rc = launch_long_sweep(dt, &lp, false, true, pdl, st, &p->launches);
+    if (rc == BLDM_OK) rc = finalize();
+    for (size_t it = 0; it < max_iter && rc == BLDM_OK; ++it) {
+        if (ev && 2 * it + 1 < nev) cudaEventRecord(ev[2 * it], st);
+        rc = launch_long_sweep(dt, &lp, true, plus_appr != 0, pdl, st, &p->launches);
+        if (ev && 2 * it + 1 < nev) cudaEventRecord(ev[2 * it + 1], st);
+        if (rc == BLDM_OK && it + 1 < max_iter) rc = finalize();
+    }
+    if (rc) return rc;
+    return cuda_status(cudaGetLastError());
+}
+
+template <typename T>
 static int run_typed(PlanImpl* p, const void* dX, const double* dalpha, const double* dbeta,
                      void* dS, size_t max_iter, int psi_mode, double eps, cudaStream_t st,
                      cudaEvent_t* ev, size_t nev) {
+    if (p->cfg.long_mode)
+        return run_long<T>(p, dX, dalpha, dbeta, dS, max_iter, psi_mode, eps, st, ev, nev);
     const SweepCfg& c = p->cfg;
     const int plus_appr = psi_mode != BLDM_PSI_EXACT;
     const int minus_appr = psi_mode == BLDM_PSI_APPR;
@@ -633,6 +756,14 @@ int plan_sums(PlanImpl* p, const void* dS, cudaStream_t st) {
     if (!p || !p->ws || !dS) return BLDM_ERR_BAD_ARG;
     if (reinterpret_cast<uintptr_t>(dS) & 15) return BLDM_ERR_BAD_ARG;
     const SweepCfg& c = p->cfg;
+    if (c.long_mode) {
+        if (p->dtype == BLDM_F64) {
+            const LongSweepParams<double> lp = long_params<double>(p, nullptr, const_cast<void*>(dS), 0.0);
+            return launch_long_sweep(BLDM_F64, &lp, false, true, false, st, &p->launches);
+        }
+        const LongSweepParams<float> lp = long_params<float>(p, nullptr, const_cast<void*>(dS), 0.0);
+        return launch_long_sweep(BLDM_F32, &lp, false, true, false, st, &p->launches);
+    }
     const dim3 grid_s(unsigned(c.n_bands) * unsigned(c.n_rr));
     if (p->dtype == BLDM_F64) {
         SweepFn<double> f = pick_sweep<double>(c, SWEEP_SUMS, true);
@@ -660,17 +791,25 @@ static int shard_step_typed(PlanImpl* p, const void* dX, void* dS, const double*
     const SweepCfg& c = p->cfg;
     const int plus_appr = psi_mode != BLDM_PSI_EXACT;
     const int minus_appr = psi_mode == BLDM_PSI_APPR;
-    SweepFn<T> f = pick_sweep<T>(c, update ? SWEEP_UPDATE : SWEEP_SUMS,
-                                 update ? plus_appr != 0 : true);
-    if (!f) return BLDM_ERR_UNSUPPORTED;
-    const SweepParams<T> sp = sweep_params<T>(p, dX, dS, eps);
     FinParams<T> fp = fin_params<T>(p, dalpha, nullptr, plus_appr, minus_appr);
     fp.f.red = d_red;
-    const dim3 grid_s(unsigned(c.n_bands) * unsigned(c.n_rr));
     const dim3 grid_f(unsigned(fp.f.nbB + fp.f.n_ablk));
-    f<<<grid_s, kSweepThreads, update ? c.smem_update : c.smem_sums, st>>>(sp);
+    if (c.long_mode) {
+        const LongSweepParams<T> lp = long_params<T>(p, dX, dS, eps);
+        const int rc = launch_long_sweep(sizeof(T) == 8 ? BLDM_F64 : BLDM_F32, &lp, update,
+                                         update ? plus_appr != 0 : true, false, st, &p->launches);
+        if (rc) return rc;
+    } else {
+        SweepFn<T> f = pick_sweep<T>(c, update ? SWEEP_UPDATE : SWEEP_SUMS,
+                                     update ? plus_appr != 0 : true);
+        if (!f) return BLDM_ERR_UNSUPPORTED;
+        const SweepParams<T> sp = sweep_params<T>(p, dX, dS, eps);
+        const dim3 grid_s(unsigned(c.n_bands) * unsigned(c.n_rr));
+        f<<<grid_s, kSweepThreads, update ? c.smem_update : c.smem_sums, st>>>(sp);
+        p->launches += 1;
+    }
     finalize_kernel<T><<<grid_f, kFinThreads, 0, st>>>(fp);
-    p->launches += 2;
+    p->launches += 1;
     return cuda_status(cudaGetLastError());
 }
 

@@ -146,7 +146,10 @@ def test_modes_match_oracle(bldm, oracle, workloads, mode):
 
 SHAPES = [(1, 1, 1), (3, 5, 1), (2, 3, 2), (33, 65, 3), (65, 33, 17), (7, 300, 5),
           (5, 7, 33), (40, 41, 64), (9, 13, 100), (4, 9, 128), (3, 5, 256), (2, 3, 255), (2, 3, 512),
-          (300, 7, 8), (17, 1000, 4)]
+          (300, 7, 8), (17, 1000, 4),
+          # fibers longer than the fused sweep's lane layout (the two-pass path):
+          # odd z above 256, even z above 512
+          (3, 5, 257), (3, 5, 513), (4, 9, 1000), (2, 3, 2048), (17, 11, 600), (70, 9, 777)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
@@ -163,7 +166,8 @@ def test_odd_shapes_fp64(bldm, oracle, shape):
 
 
 @pytest.mark.parametrize("shape", [(3, 5, 1), (33, 65, 3), (40, 41, 4), (9, 13, 64), (5, 7, 17),
-                                   (64, 48, 8), (4, 9, 512), (3, 4, 1000)])
+                                   (64, 48, 8), (4, 9, 512), (3, 4, 1000),
+                                   (3, 4, 1500), (6, 10, 1025), (5, 3, 301)])
 def test_odd_shapes_fp32(bldm, oracle, shape):
     x, y, z = shape
     rng = np.random.default_rng(x * 7 + y * 13 + z)
@@ -180,6 +184,33 @@ def test_odd_shapes_fp32(bldm, oracle, shape):
     ref32 = oracle.bld_mult(X, z, alpha, beta, 12, oracle.PSI_APPR, 1e-50, S0=S0,
                             dtype=np.float32)
     assert rel_err(S, ref) <= max(1e-5, 10 * rel_err(ref32, ref))
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_long_fibers_all_modes_match_oracle(bldm, oracle, mode):
+    """The two-pass long-fiber path in every digamma mode, with rows of X that
+    are all zero and fibers of several k-chunks, bands and row ranges."""
+    rng = np.random.default_rng(90 + mode)
+    x, y, z = 45, 21, 1100
+    X = rng.poisson(3.0, (x, y)).astype(np.float64)
+    X[7, :] = 0.0
+    X[:, 4] = 0.0
+    alpha = rng.uniform(0.5, 2, x)
+    beta = rng.uniform(0.5, 2, z)
+    S0 = oracle.init_S(X, z, 4)
+    ref = oracle.bld_mult(X, z, alpha, beta, 15, mode, 1e-50, S0=S0)
+    params = bldm.Params(1.0, 1.0, alpha, beta)
+    stats = {}
+    S = bldm._solve(X, z, params, 15, mode, 1e-50, S0, 0, bldm.F64, stats)
+    assert rel_err(S, ref) <= 1e-9
+    assert np.all(S[X == 0] == 0)
+    want = float((np.abs(S.sum(axis=2) - X) / np.maximum(X, 1.0)).max())
+    assert abs(stats["conservation_residual"] - want) <= 1e-12 * max(want, 1.0)
+    # bld_fact of the long-fiber solution (the sums sweep of the same path)
+    W0, H0, L0 = oracle.bld_fact(S, alpha, beta, 1.0, 1.0, 1e-50)
+    W, H, L = bldm.bld_fact(S, params)
+    for a, b in ((W, W0), (H, H0), (L, L0)):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
 
 
 def test_fp32_plain_small_vs_fp64_oracle(bldm, plain_small_golden):

@@ -4,10 +4,11 @@ It serves callers that cannot allocate device memory while they solve (a
 serving loop that must not let cudaMalloc/cudaFree synchronise the device, a
 process whose HBM another allocator already holds).  Its scratch is a fixed
 32 MiB array in the library's device data.  This test calls it through the C
-ABI on device buffers that the test itself allocates, twice in a row with
-different inputs (the array keeps the previous call's contents), and compares
-each result with the plan API's (bldm_plan_run) at the solver tests'
-tolerance (1e-9 max-norm relative for FP64, 1e-5 for FP32).  This file is
+ABI on device buffers that the test itself allocates, three times in a row
+with different inputs (the array keeps the previous call's contents; the third
+shape has fibers longer than the fused sweep's lane layout), and compares each
+result with the plan API's (bldm_plan_run) at the solver tests' tolerance
+(1e-9 max-norm relative for FP64, 1e-5 for FP32).  This file is
 named so that pytest collects it last.
 """
 
@@ -44,7 +45,8 @@ def _rel(a, b):
 @pytest.mark.parametrize("dtype,tol", [(0, 1e-9), (1, 1e-5)])
 def test_noalloc_matches_plan_api_twice(bldm, workloads, oracle, dtype, tol):
     tt = torch.float64 if dtype == bldm.F64 else torch.float32
-    for call, (seed, x, y, z, iters) in enumerate([(1, 96, 80, 16, 30), (2, 130, 70, 8, 25)]):
+    for call, (seed, x, y, z, iters) in enumerate([(1, 96, 80, 16, 30), (2, 130, 70, 8, 25),
+                                                   (3, 20, 12, 1300, 6)]):
         X, S0 = _problem(workloads, oracle, seed, x, y, z)
         dX = torch.as_tensor(X).to("cuda", tt)
         da = torch.ones(x, dtype=torch.float64, device="cuda")
