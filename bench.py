@@ -690,6 +690,25 @@ def batch_measure(pkg, torch, args, steps, loop_reps=2, autotune=True):
     b.check(stream)
     ms = e0.elapsed_time(e1) / steps
     launches = b.info()["launches"] - l0
+    # the same runs in the persistent form (one launch per class for a whole
+    # run), for comparison; S continues
+    persist = None
+    b.set_launch_mode(True)
+    if b.persistent():
+        b.run(iters, pkg.PSI_APPR, 1e-50, True, stream)
+        n_p = max(2, steps // 3)
+        lp0 = b.info()["launches"]
+        e0.record(stream)
+        for _ in range(n_p):
+            b.run(iters, pkg.PSI_APPR, 1e-50, True, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        b.check(stream)
+        p_ms = e0.elapsed_time(e1) / n_p
+        persist = {"ms_per_step": p_ms, "solves_per_s": len(shapes) / (p_ms / 1e3),
+                   "steps": n_p, "gpu_launches_per_run": (b.info()["launches"] - lp0) / n_p,
+                   "vs_per_iteration_form": ms / p_ms}
+    b.set_launch_mode(False)
     cons = b.conservation(stream)
     # loop of the plain per-instance solver (one plan per distinct shape)
     plans = {}
@@ -735,6 +754,8 @@ def batch_measure(pkg, torch, args, steps, loop_reps=2, autotune=True):
            "speedup_vs_plain_loop": loop_ms / ms,
            "conservation_residual_max": float(np.max(cons)),
            "conservation_residual_median": float(np.median(cons)),
+           "launch_form": "per iteration: a sweep launch per class, one finalize launch",
+           "persistent_form": persist,
            "classes": b.info()["classes"], "gpu_launches": launches,
            "gpu_launches_per_solve_iteration": launches / (steps * iters),
            "setup_s": setup_s, "autotune": tune, "clocks": clk.summary()}

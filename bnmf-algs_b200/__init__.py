@@ -192,6 +192,9 @@ SIGNATURES = {
     "bldm_batch_run": (ctypes.c_int, [_vp, _sz, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                       _vp]),
     "bldm_batch_check": (ctypes.c_int, [_vp, _vp]),
+    "bldm_batch_set_launch_mode": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.c_int]),
+    "bldm_batch_get_launch_mode": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "bldm_batch_get": (ctypes.c_int, [_vp, _sz, _dp, _dp]),
     "bldm_batch_conservation": (ctypes.c_int, [_vp, _dp, _vp]),
     "bldm_batch_device_ptrs": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp),
@@ -594,6 +597,17 @@ class Batch:
 
     def check(self, stream=None):
         _check(lib().bldm_batch_check(self._h, _stream_ptr(stream)), "batch_check")
+
+    def set_launch_mode(self, persistent=True, wait_limit_s=1.0, stall_test=False):
+        """Persistent launches per class (default) or one launch per class and iteration."""
+        _check(lib().bldm_batch_set_launch_mode(self._h, 1 if persistent else 0,
+                                                float(wait_limit_s), 1 if stall_test else 0),
+               "batch_set_launch_mode")
+
+    def persistent(self):
+        v = ctypes.c_int()
+        _check(lib().bldm_batch_get_launch_mode(self._h, ctypes.byref(v)))
+        return bool(v.value)
 
     def get(self, idx):
         x, y, z = self.shapes[idx]

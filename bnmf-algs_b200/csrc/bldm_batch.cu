@@ -87,7 +87,7 @@ int bldm_batch_create(bldm_batch** out, int dtype, size_t n, const size_t* xs, c
         b->ptrs[i] = &b->inst[i];
     }
     for (size_t i = 0; i < n; ++i) {
-        e = cudaMemset(b->inst[i].counter, 0, 16);
+        e = cudaMemset(b->inst[i].counter, 0, b->eng->bytes(b->inst[i]).counter);
         // empty row lists until bldm_batch_set fills them from X
         if (e == cudaSuccess)
             e = cudaMemset(b->inst[i].nz_cnt, 0, b->eng->bytes(b->inst[i]).nzc);
@@ -142,6 +142,20 @@ int bldm_batch_run(bldm_batch* b, size_t iters, int psi_mode, double eps, int us
                                static_cast<cudaStream_t>(stream), true, b->clean);
     if (rc == BLDM_OK && iters > 0) b->clean = true;
     return rc;
+}
+
+int bldm_batch_set_launch_mode(bldm_batch* b, int persistent, double wait_limit_s,
+                               int stall_test) {
+    if (!b || !(wait_limit_s > 0.0) || wait_limit_s > 60.0) return BLDM_ERR_BAD_ARG;
+    b->eng->set_persistent(persistent != 0, (unsigned long long)(wait_limit_s * 1e9),
+                           stall_test != 0);
+    return BLDM_OK;
+}
+
+int bldm_batch_get_launch_mode(const bldm_batch* b, int* persistent) {
+    if (!b || !persistent) return BLDM_ERR_BAD_ARG;
+    *persistent = b->eng->persistent_active() ? 1 : 0;
+    return BLDM_OK;
 }
 
 int bldm_batch_check(bldm_batch* b, void* stream) {

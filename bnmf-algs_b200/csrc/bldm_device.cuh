@@ -357,6 +357,41 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     }
 }
 
+// Invalidates an mbarrier whose phases have all completed, so that its shared
+// memory can hold a new mbarrier (a persistent CTA re-initialises its ring for
+// every tile).
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Acquire load of a counter written by other CTAs (gpu scope).
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Orders this thread's generic-proxy accesses (and what they synchronised
+// with) before its later bulk copies (async proxy), and the reverse.
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+// Waits until *ctr >= target: false after limit_ns of %globaltimer or when
+// *abort is set.  One thread calls it.
+__device__ __forceinline__ bool wait_counter_bounded(const unsigned* ctr, unsigned target,
+                                                     const unsigned* abort,
+                                                     unsigned long long limit_ns) {
+    if (ld_acquire_gpu(ctr) >= target) return true;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        if (ld_acquire_gpu(ctr) >= target) return true;
+        if (ld_acquire_gpu(abort) != 0u) return false;
+        if (global_ns() - t0 > limit_ns) return false;
+        __nanosleep(64);
+    }
+}
+
 __device__ __forceinline__ uint64_t policy_evict_first() {
     uint64_t p;
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));

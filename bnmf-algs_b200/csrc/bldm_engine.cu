@@ -3,12 +3,15 @@
 #include <cstring>
 
 #include "bldm_engine.h"
+#include "bldm_finalize.cuh"
 
 namespace bldm {
 
 namespace {
 
 size_t a256(size_t v) { return (v + 255) & ~size_t(255); }
+
+
 
 int sms_of_current_device() {
     int dev = 0, n = 0;
@@ -44,6 +47,7 @@ Engine::Engine(int dtype, int rows_per_tile, bool skip_zero)
 Engine::~Engine() {
     drop_graphs();
     free_tables();
+    if (d_counters_) cudaFree(d_counters_);
     for (auto& c : classes_) {
         if (c.stream) cudaStreamDestroy(c.stream);
         if (c.done) cudaEventDestroy(c.done);
@@ -71,6 +75,7 @@ int Engine::configure(EngineInstance& in, size_t x, size_t y, size_t z) const {
     retile(in);
     const SlotLayout lay((long long)c.band_w, (long long)z, int(es_));
     in.stage_need = uint32_t(rps) * (lay.capS + lay.capX + lay.capA);
+    // finalize launch geometry (the per-iteration form)
     const int KT = int(std::min<size_t>(z, kFinThreads));
     const int Rf = kFinThreads / KT;
     const long rows = std::max<long>(Rf, long((x + 127) / 128));
@@ -138,8 +143,11 @@ InstanceBytes Engine::bytes(const EngineInstance& in) const {
     b.psiB = in.y * in.z * es_;
     b.psiA = in.x * in.z * es_;
     b.psiAS = in.z * es_;
-    b.asum = size_t(c.n_ablk) * in.z * 8;
-    b.counter = 16;
+    // sums of alpha_eph over row blocks (finalize launch) or row ranges (fused
+    // finalize), and the last-arrival counters: word 0 of the finalize launch,
+    // or instance | per band | per row range of the fused finalize
+    b.asum = size_t(std::max(c.n_ablk, in.rr_cap)) * in.z * 8;
+    b.counter = std::max<size_t>(16, (1 + size_t(c.n_bands) + size_t(in.rr_cap)) * sizeof(unsigned));
     b.delta = size_t(in.rr_cap) * c.n_bands * 16;
     b.rel = 8;
     b.nzr = size_t(c.n_bands) * in.x * 4;
@@ -219,6 +227,12 @@ static void fill_tables(const std::vector<EngineInstance*>& insts, std::vector<c
         s.n_rr = c.n_rr;
         s.rr_base = c.rr_base;
         s.rr_extra = c.rr_extra;
+        s.alpha = in.alpha;
+        s.beta = in.beta;
+        s.fcnt = in.counter;
+        s.asum_rr = in.asum;
+        s.rel_change = in.rel;
+        s.done = nullptr;
         FinInst<T>& f = fi[n];
         f.red = nullptr;
         f.part_pjk = in.part_pjk;
@@ -297,6 +311,8 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
         const ClassTune t = tune_of(ClassKey{k.vec, k.lpf, k.mch, k.multirow});
         if (t.stages >= 2) k.stages = std::min(k.stages, t.stages);
         k.smem = size_t(k.stages) * per_stage + fixed;
+        // a persistent launch's finalize items keep their row sums in the ring
+        k.smem = std::max(k.smem, size_t(kFinAccDoubles) * sizeof(double));
         for (int mode = SWEEP_SUMS; mode <= SWEEP_COMPACT; ++mode)
             for (int ap = 0; ap < 2; ++ap) {
                 void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, mode, ap != 0, true,
@@ -334,8 +350,50 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
         std::stable_sort(k.tiles.begin(), k.tiles.end(),
                          [&](const BatchTile& a, const BatchTile& b) { return work(a) > work(b); });
     }
-    // Device tables: SweepInst[n] | FinInst[n] | block_off[n+1] | err | tiles per class.
+    // Persistent launches: every class needs its persistent kernel (short
+    // fibers); a round of a class is its tiles in the order above.
     const size_t n = insts.size();
+    persist_ok_ = !classes_.empty();
+    for (auto& k : classes_) {
+        k.items.clear();
+        for (int ap = 0; ap < 2; ++ap)
+            k.pfn[ap] = pick_persist_fn(dtype_, k.vec, k.lpf, k.mch, k.multirow, ap != 0);
+        if (!k.pfn[0] || !k.pfn[1]) {
+            persist_ok_ = false;
+            continue;
+        }
+        for (const BatchTile& bt : k.tiles) k.items.push_back(PItem{0, bt.inst, bt.band, bt.rr});
+        for (int ap = 0; ap < 2; ++ap) {
+            const int rc_attr = ensure_smem_attr(k.pfn[ap], k.smem);
+            if (rc_attr) return rc_attr;
+        }
+    }
+    if (persist_ok_) {
+        // Every class's launch gets one wave of CTAs (at most one round's
+        // tiles); launched side by side, a later class takes the SMs as an
+        // earlier one drains.  (Measured: splitting one wave between the classes
+        // in proportion to their bytes starves the classes of small instances,
+        // whose rounds are bound by latency, not bytes.)
+        for (auto& k : classes_) {
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.pfn[1], kSweepThreads,
+                                                              k.smem) != cudaSuccess ||
+                per_sm < 1)
+                per_sm = 1;
+            const long cap = long(per_sm) * num_sms_;
+            k.grid = int(std::max(1L, std::min(cap, long(k.items.size()))));
+        }
+        const size_t cb = (n + 4 * classes_.size()) * sizeof(unsigned);
+        if (cb > counter_bytes_) {
+            if (d_counters_) cudaFree(d_counters_);
+            d_counters_ = nullptr;
+            counter_bytes_ = 0;
+            ENG_CU(cudaMalloc(&d_counters_, cb * 2));
+            counter_bytes_ = cb * 2;
+        }
+    }
+    // Device tables: SweepInst[n] | FinInst[n] | block_off[n+1] | err | tiles per
+    // class | (persistent) items per class.
     const size_t s_sz = dtype_ == BLDM_F64 ? sizeof(SweepInst<double>) : sizeof(SweepInst<float>);
     const size_t f_sz = dtype_ == BLDM_F64 ? sizeof(FinInst<double>) : sizeof(FinInst<float>);
     const size_t o_sinst = 0;
@@ -343,10 +401,14 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
     const size_t o_boff = a256(o_finst + n * f_sz);
     const size_t o_err = a256(o_boff + (n + 1) * sizeof(int));
     size_t off = a256(o_err + 64);
-    std::vector<size_t> o_tiles(classes_.size());
+    std::vector<size_t> o_tiles(classes_.size()), o_items(classes_.size());
     for (size_t c = 0; c < classes_.size(); ++c) {
         o_tiles[c] = off;
         off = a256(off + classes_[c].tiles.size() * sizeof(BatchTile));
+    }
+    for (size_t c = 0; c < classes_.size(); ++c) {
+        o_items[c] = off;
+        off = a256(off + classes_[c].items.size() * sizeof(PItem));
     }
     table_bytes_ = off;
     if (table_bytes_ > h_cap_) {
@@ -388,7 +450,11 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
         std::memcpy(host + o_tiles[c], classes_[c].tiles.data(),
                     classes_[c].tiles.size() * sizeof(BatchTile));
         classes_[c].d_tiles = reinterpret_cast<BatchTile*>(base + o_tiles[c]);
+        std::memcpy(host + o_items[c], classes_[c].items.data(),
+                    classes_[c].items.size() * sizeof(PItem));
+        classes_[c].d_items = reinterpret_cast<PItem*>(base + o_items[c]);
     }
+
     d_sinst_ = base + o_sinst;
     d_finst_ = base + o_finst;
     d_block_off_ = reinterpret_cast<int*>(base + o_boff);
@@ -401,7 +467,8 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
 template <typename T>
 static void launch_class_kernel(void* fn, unsigned grid, size_t smem, cudaStream_t s,
                                 const void* d_sinst, const BatchTile* d_tiles, int stages,
-                                uint32_t stage_bytes, double eps, int* err, bool track) {
+                                uint32_t stage_bytes, double eps, int* err, bool track,
+                                int plus_appr, int minus_appr) {
     BatchSweepParams<T> p;
     p.insts = static_cast<const SweepInst<T>*>(d_sinst);
     p.tiles = d_tiles;
@@ -409,12 +476,18 @@ static void launch_class_kernel(void* fn, unsigned grid, size_t smem, cudaStream
     p.L.stage_bytes = stage_bytes;
     p.L.eps = eps;
     p.L.err = err;
+    p.L.plus_appr = plus_appr;
+    p.L.minus_appr = minus_appr;
     p.track = track ? 1 : 0;
     reinterpret_cast<void (*)(const BatchSweepParams<T>)>(fn)<<<grid, kSweepThreads, smem, s>>>(p);
 }
 
-int Engine::launch_sweeps(bool update, bool appr, bool track, double eps, cudaStream_t st,
+// The sweeps of one round of every instance: a launch per class, the classes
+// side by side on forked streams.
+int Engine::launch_sweeps(bool update, int psi_mode, bool track, double eps, cudaStream_t st,
                           bool clean) {
+    const int plus_appr = psi_mode != BLDM_PSI_EXACT;
+    const int minus_appr = psi_mode == BLDM_PSI_APPR;
     const bool fork = classes_.size() > 1;
     if (fork) ENG_CU(cudaEventRecord(fork_, st));
     for (auto& k : classes_) {
@@ -422,13 +495,16 @@ int Engine::launch_sweeps(bool update, bool appr, bool track, double eps, cudaSt
         cudaStream_t s = fork ? k.stream : st;
         if (fork) ENG_CU(cudaStreamWaitEvent(s, fork_, 0));
         const int mode = !update ? SWEEP_SUMS : (clean ? SWEEP_COMPACT : SWEEP_UPDATE);
-        void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, mode, appr, true, k.multirow);
+        void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, mode, plus_appr != 0, true,
+                                 k.multirow);
         if (dtype_ == BLDM_F64)
             launch_class_kernel<double>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_,
-                                        k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track);
+                                        k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track,
+                                        plus_appr, minus_appr);
         else
             launch_class_kernel<float>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_,
-                                       k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track);
+                                       k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track,
+                                       plus_appr, minus_appr);
         ENG_CU(cudaGetLastError());
         launches_ += 1;
         if (fork) ENG_CU(cudaEventRecord(k.done, s));
@@ -452,7 +528,10 @@ static void launch_fin_kernel(unsigned grid, cudaStream_t s, const void* d_finst
     reinterpret_cast<void (*)(const BatchFinParams<T>)>(fn)<<<grid, kFinThreads, 0, s>>>(p);
 }
 
-int Engine::launch_finalize(int plus_appr, int minus_appr, cudaStream_t st) {
+// The finalize of every instance in one launch (block_off maps blocks to instances).
+int Engine::launch_finalize(int psi_mode, cudaStream_t st) {
+    const int plus_appr = psi_mode != BLDM_PSI_EXACT;
+    const int minus_appr = psi_mode == BLDM_PSI_APPR;
     if (dtype_ == BLDM_F64)
         launch_fin_kernel<double>(unsigned(fin_blocks_), st, d_finst_, d_block_off_,
                                   int(insts_.size()), plus_appr, minus_appr);
@@ -466,27 +545,90 @@ int Engine::launch_finalize(int plus_appr, int minus_appr, cudaStream_t st) {
 int Engine::prime(int psi_mode, cudaStream_t st) {
     if (psi_mode < BLDM_PSI_EXACT || psi_mode > BLDM_PSI_LEGACY_CUDA) return BLDM_ERR_BAD_ARG;
     if (insts_.empty()) return BLDM_OK;
-    const int rc = launch_sweeps(false, true, false, 0.0, st, false);
+    const int rc = launch_sweeps(false, psi_mode, false, 0.0, st, false);
     if (rc) return rc;
-    return launch_finalize(psi_mode != BLDM_PSI_EXACT, psi_mode == BLDM_PSI_APPR, st);
+    return launch_finalize(psi_mode, st);
+}
+
+template <typename T>
+static int launch_persist_class(void* fn, int grid, size_t smem, cudaStream_t s,
+                                const PersistParams<T>& p) {
+    reinterpret_cast<void (*)(const PersistParams<T>)>(fn)<<<grid, kSweepThreads, smem, s>>>(p);
+    return cuda_status(cudaGetLastError());
+}
+
+// One launch per class for the whole run (rounds = prime round + iters).
+int Engine::launch_persistent(size_t iters, int psi_mode, double eps, cudaStream_t st,
+                              bool prime, bool clean_first) {
+    const int plus_appr = psi_mode != BLDM_PSI_EXACT;
+    const int minus_appr = psi_mode == BLDM_PSI_APPR;
+    const size_t n = insts_.size();
+    const int rounds = int(iters) + (prime ? 1 : 0);
+    unsigned* ctr = static_cast<unsigned*>(d_counters_);
+    ENG_CU(cudaMemsetAsync(ctr, 0, (n + 4 * classes_.size()) * sizeof(unsigned), st));
+    const bool fork = classes_.size() > 1;
+    if (fork) ENG_CU(cudaEventRecord(fork_, st));
+    for (size_t c = 0; c < classes_.size(); ++c) {
+        ShapeClass& k = classes_[c];
+        if (k.items.empty()) continue;
+        cudaStream_t s = fork ? k.stream : st;
+        if (fork) ENG_CU(cudaStreamWaitEvent(s, fork_, 0));
+        int rc;
+        auto fill = [&](auto& p) {
+            p.items = k.d_items;
+            p.done = ctr;
+            p.ctl = reinterpret_cast<PersistCtl*>(ctr + n) + c;
+            p.L.stages = k.stages;
+            p.L.stage_bytes = k.stage_bytes;
+            p.L.eps = eps;
+            p.L.err = d_err_;
+            p.L.plus_appr = plus_appr;
+            p.L.minus_appr = minus_appr;
+            p.P = int(k.items.size());
+            p.rounds = rounds;
+            p.prime = prime ? 1 : 0;
+            p.compact_from = !skip_zero_ ? rounds : (prime ? 1 : 0) + (clean_first ? 0 : 1);
+            p.wait_ns = wait_ns_;
+            p.stall_test = stall_test_ ? 1 : 0;
+        };
+        void* fn = k.pfn[plus_appr ? 1 : 0];
+        if (dtype_ == BLDM_F64) {
+            PersistParams<double> p;
+            p.sinst = static_cast<const SweepInst<double>*>(d_sinst_);
+            fill(p);
+            rc = launch_persist_class<double>(fn, k.grid, k.smem, s, p);
+        } else {
+            PersistParams<float> p;
+            p.sinst = static_cast<const SweepInst<float>*>(d_sinst_);
+            fill(p);
+            rc = launch_persist_class<float>(fn, k.grid, k.smem, s, p);
+        }
+        if (rc) return rc;
+        launches_ += 1;
+        if (fork) ENG_CU(cudaEventRecord(k.done, s));
+    }
+    if (fork)
+        for (auto& k : classes_)
+            if (!k.items.empty()) ENG_CU(cudaStreamWaitEvent(st, k.done, 0));
+    return BLDM_OK;
 }
 
 int Engine::launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st,
                             bool prime, bool clean_first) {
-    const int plus_appr = psi_mode != BLDM_PSI_EXACT;
-    const int minus_appr = psi_mode == BLDM_PSI_APPR;
+    if (persistent_active())
+        return launch_persistent(iters, psi_mode, eps, st, prime, clean_first);
     int rc = BLDM_OK;
     if (prime) {
-        rc = launch_sweeps(false, true, false, eps, st, false);
+        rc = launch_sweeps(false, psi_mode, false, eps, st, false);
         if (rc) return rc;
-        rc = launch_finalize(plus_appr, minus_appr, st);
+        rc = launch_finalize(psi_mode, st);
         if (rc) return rc;
     }
     for (size_t it = 0; it < iters; ++it) {
         const bool clean = skip_zero_ && (clean_first || it > 0);
-        rc = launch_sweeps(true, plus_appr != 0, it + 1 == iters, eps, st, clean);
+        rc = launch_sweeps(true, psi_mode, it + 1 == iters, eps, st, clean);
         if (rc) return rc;
-        rc = launch_finalize(plus_appr, minus_appr, st);
+        rc = launch_finalize(psi_mode, st);
         if (rc) return rc;
     }
     return BLDM_OK;
@@ -521,7 +663,8 @@ int Engine::run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStre
         it = graphs_.emplace(key, exec).first;
     }
     ENG_CU(cudaGraphLaunch(it->second, st));
-    launches_ += (iters + (prime ? 1 : 0)) * (classes_.size() + 1);
+    launches_ += persistent_active() ? classes_.size()
+                                     : (iters + (prime ? 1 : 0)) * (classes_.size() + 1);
     return BLDM_OK;
 }
 
@@ -529,9 +672,15 @@ int Engine::check(cudaStream_t st) {
     ENG_CU(cudaStreamSynchronize(st));
     if (!d_err_) return BLDM_OK;
     int herr = 0;
-    ENG_CU(cudaMemcpy(&herr, d_err_, sizeof(int), cudaMemcpyDeviceToHost));
+    ENG_CU(cudaMemcpyAsync(&herr, d_err_, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ENG_CU(cudaStreamSynchronize(st));
     if (herr) {
-        ENG_CU(cudaMemset(d_err_, 0, sizeof(int)));
+        // A run that gave up may have left an instance's finalize half counted:
+        // clear every instance's last-block counter with the error word.
+        ENG_CU(cudaMemsetAsync(d_err_, 0, sizeof(int), st));
+        for (EngineInstance* in : insts_)
+            ENG_CU(cudaMemsetAsync(in->counter, 0, bytes(*in).counter, st));
+        ENG_CU(cudaStreamSynchronize(st));
         return BLDM_ERR_TIMEOUT;
     }
     return BLDM_OK;

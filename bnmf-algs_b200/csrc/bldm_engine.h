@@ -4,7 +4,9 @@
 //
 // An iteration of every instance is one sweep launch per lane-shape class
 // (instances whose z maps to the same kernel), the classes running
-// concurrently on forked streams, then one finalize launch for all instances.
+// concurrently on forked streams, then one finalize launch for all instances;
+// or, persistent, one launch per class for a whole run whose tiles finalize
+// their instances in their epilogues.
 // Tiles (band x row range) of every instance of a class form the class grid;
 // the tiling of an instance depends only on its own shape, so its results do
 // not depend on which other instances share the launches.
@@ -45,7 +47,7 @@ struct EngineInstance {
     size_t x = 0, y = 0, z = 0;
     SweepCfg cfg{};      // lane shape, wpr, band_w, n_bands, n_rr, rr_base, n_ablk...
     int rr_cap = 0;      // row ranges the partial buffers hold (any tile height >= kMinTileRows)
-    int nbB = 0;         // finalize blocks for psi(beta_eph)
+    int nbB = 0;         // finalize-launch blocks for psi(beta_eph)
     uint32_t stage_need = 0;
     // device buffers (owned by the engine's user)
     void* X = nullptr;
@@ -57,8 +59,8 @@ struct EngineInstance {
     void* psiB = nullptr;
     void* psiA = nullptr;
     void* psiAS = nullptr;
-    double* asum = nullptr;
-    unsigned* counter = nullptr;
+    double* asum = nullptr;       // [rr_cap][z] fused finalize: alpha_eph summed per row range
+    unsigned* counter = nullptr;  // [1 + n_bands + rr_cap] fused finalize arrival counters
     double* delta = nullptr;
     double* rel = nullptr;
     int* nz_rows = nullptr;  // [n_bands][x] rows with X != 0 per band, ascending
@@ -118,6 +120,20 @@ class Engine {
     int prime(int psi_mode, cudaStream_t st);
     int check(cudaStream_t st);
 
+    // Persistent launches (one per class for a whole run; bldm_persist.cuh)
+    // instead of one launch per class and round (the default, faster on mixes
+    // of small instances).  Used when every class has a persistent kernel;
+    // wait_ns bounds each dependency wait; stall_test makes instance 0's
+    // first-round tiles wait for a round that cannot complete before them
+    // (failure-detection tests).
+    void set_persistent(bool on, unsigned long long wait_ns, bool stall_test) {
+        persistent_ = on;
+        wait_ns_ = wait_ns;
+        stall_test_ = stall_test;
+        drop_graphs();
+    }
+    bool persistent_active() const { return persistent_ && persist_ok_; }
+
     int dtype() const { return dtype_; }
     size_t es() const { return es_; }
     size_t n_classes() const { return classes_.size(); }
@@ -136,12 +152,19 @@ class Engine {
         BatchTile* d_tiles = nullptr;
         cudaStream_t stream = nullptr;
         cudaEvent_t done = nullptr;
+        // persistent launch of the class
+        void* pfn[2] = {nullptr, nullptr};  // by digamma of grad_plus: exact, psi_appr
+        std::vector<PItem> items;  // one round: the tiles, largest first
+        PItem* d_items = nullptr;
+        int grid = 0;
     };
+    int launch_persistent(size_t iters, int psi_mode, double eps, cudaStream_t st, bool prime,
+                          bool clean_first);
     int launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st, bool prime,
                         bool clean_first);
-    int launch_sweeps(bool update, bool appr, bool track, double eps, cudaStream_t st,
+    int launch_sweeps(bool update, int psi_mode, bool track, double eps, cudaStream_t st,
                       bool clean);
-    int launch_finalize(int plus_appr, int minus_appr, cudaStream_t st);
+    int launch_finalize(int psi_mode, cudaStream_t st);
     void free_tables();
     void drop_graphs();
 
@@ -152,7 +175,7 @@ class Engine {
     int num_sms_;
     std::vector<EngineInstance*> insts_;
     std::vector<ShapeClass> classes_;
-    void* d_tables_ = nullptr;  // SweepInst[n] | FinInst[n] | block_off[n+1] | err | tiles
+    void* d_tables_ = nullptr;  // SweepInst[n] | FinInst[n] | block_off[n+1] | err | tiles | items
     size_t table_bytes_ = 0;    // bytes in use
     size_t table_cap_ = 0;      // bytes allocated (grow-only across builds)
     void* h_stage_ = nullptr;   // pinned host staging of the tables
@@ -160,11 +183,19 @@ class Engine {
     void* d_sinst_ = nullptr;
     void* d_finst_ = nullptr;
     int* d_block_off_ = nullptr;
-    int* d_err_ = nullptr;
     int fin_blocks_ = 0;
+    int* d_err_ = nullptr;
     cudaEvent_t fork_ = nullptr;
     uint64_t launches_ = 0;
     std::map<std::tuple<size_t, int, uint64_t, bool, bool>, cudaGraphExec_t> graphs_;
+    // persistent launches: the counters cleared before every run (rounds done
+    // per instance [n] | queue control per class)
+    bool persistent_ = false;
+    bool persist_ok_ = false;
+    bool stall_test_ = false;
+    unsigned long long wait_ns_ = 1000000000ull;
+    void* d_counters_ = nullptr;
+    size_t counter_bytes_ = 0;
     std::map<ClassKey, ClassTune> tune_;
 };
 

@@ -36,14 +36,28 @@ template <typename T> struct SweepInst {
     long long x, y, z;
     int n_bands, band_w, wpr;
     int n_rr, rr_base, rr_extra;
+    // Finalize in the tiles' epilogue (multi-instance sweeps, tile_finalize in
+    // bldm_finalize.cuh): the last tile of a band tabulates the band's
+    // psi(beta_eph), the last tile of a row range its rows' psi(alpha_eph) and
+    // their sum over the rows, the last tile of the instance psi(sum_i
+    // alpha_eph) and the relative change.  Unused by the single-instance plan.
+    const double* alpha;   // [x]
+    const double* beta;    // [z]
+    unsigned* fcnt;        // [1 + n_bands + n_rr] arrivals: instance | per band | per row range
+    double* asum_rr;       // [n_rr][z] sum of alpha_eph over a row range's rows
+    double* rel_change;    // sum |S_new - S| / sum |S_new| of a tracked sweep
+    unsigned* done;        // rounds the instance completed (persistent launches) or null
 };
 
-// Launch-wide constants: ring depth, bytes per stage, eps, error word.
+// Launch-wide constants: ring depth, bytes per stage, eps, error word, and the
+// digamma of the fused finalize (grad_plus's psi(beta_eph), grad_minus's
+// psi(alpha_eph)).
 struct SweepLaunch {
     int stages;
     uint32_t stage_bytes;
     double eps;
     int* err;
+    int plus_appr, minus_appr;
 };
 
 template <typename T> struct SweepParams {
@@ -109,6 +123,40 @@ template <typename T> struct BatchFinParams {
     int n_inst;
     int plus_appr, minus_appr;
 };
+
+
+// Persistent multi-instance launch (bldm_persist.cuh): one launch per lane-shape
+// class runs every round (iteration) of every instance of the class from an
+// ordered work queue of the class's sweep tiles, round after round; item q of
+// the queue is items[q % P] in round q / P.  A tile of round r waits until its
+// instance has completed r rounds (the fused finalize of the instance's last
+// tile of a round publishes it).  Every wait points to earlier items of the
+// queue, held by CTAs that are running, so the queue always drains.
+struct PItem {
+    int kind;  // reserved (0)
+    int inst;  // instance index (into the engine's instance tables)
+    int a, b;  // band, row range of the tile
+};
+struct PersistCtl {
+    unsigned next;   // queue head
+    unsigned abort;  // set when a wait gave up: every CTA stops taking items
+    unsigned pad[2];
+};
+template <typename T> struct PersistParams {
+    const SweepInst<T>* sinst;
+    const PItem* items;     // [P] one round of the class's tiles, largest first
+    unsigned* done;         // [n_inst] rounds completed per instance (cleared before the launch)
+    PersistCtl* ctl;        // this class's queue (cleared before the launch)
+    SweepLaunch L;          // ring depth and bytes per stage of the class, eps, error word
+    int P;                  // items per round
+    int rounds;             // prime round (if any) + update rounds
+    int prime;              // round 0 takes the axis sums of the current S
+    int compact_from;       // first update round that may skip zero rows (rounds if none)
+    unsigned long long wait_ns;  // limit of a dependency wait
+    int stall_test;         // test: instance 0's round-0 tiles wait for that round's completion
+};
+// The persistent kernel of a lane shape (nullptr when not instantiated).
+void* pick_persist_fn(int dtype, int vec, int lpf, int mch, bool multirow, bool appr);
 
 // Long fibers (depths beyond the fused sweep's lane layout; bldm_long.cu):
 // tiles of (k-chunk of kLongThreads, band of kLongBand columns, row range).

@@ -179,7 +179,7 @@ int bldm_server::admit(Lane& L, Request* r) {
     }
     eng->bind(r->inst, r->dmem);
     r->inst.rel = d_rel + r->slot;
-    e = cudaMemsetAsync(r->inst.counter, 0, 16, stream);
+    e = cudaMemsetAsync(r->inst.counter, 0, eng->bytes(r->inst).counter, stream);
     if (e == cudaSuccess)
         e = eng->es() == 8 ? cudaMemcpyAsync(r->inst.X, r->X.data(), r->x * r->y * 8,
                                              cudaMemcpyHostToDevice, stream)

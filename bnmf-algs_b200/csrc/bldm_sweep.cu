@@ -26,146 +26,17 @@
 
 #include "bldm_device.cuh"
 #include "bldm_internal.h"
+#include "bldm_finalize.cuh"
 #include "bldm_kernels.h"
 
 namespace bldm {
-
-// Sum of p[r * stride], r < n, in increasing r (the order of a plain loop),
-// with the loads of W terms issued before their adds so that a thread keeps W
-// reads of the partial buffers in flight (the partials were just written, so
-// the finalize waits on L2 round trips, not on bandwidth).  Terms past n load
-// nothing and add an exact 0.0.  W = 16 for the single-instance finalize (few
-// blocks, long sums); 8 for the multi-instance one, whose tens of thousands of
-// short blocks need the occupancy that fewer registers give.
-template <bool CG, int W>
-__device__ __forceinline__ double sum_strided(const double* p, long long stride, int n) {
-    double s = 0.0;
-    for (int r = 0; r < n; r += W) {
-        double v[W];
-#pragma unroll
-        for (int u = 0; u < W; ++u) {
-            const double* a = p + (long long)(r + u) * stride;
-            v[u] = (r + u < n) ? (CG ? __ldcg(a) : *a) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < W; ++u) s += v[u];
-    }
-    return s;
-}
-
-// Block `blk` of an instance's finalize.  Blocks [0, nbB): psi(beta_eph) for
-// every (j,k).  Blocks [nbB, nbB + n_ablk): psi(alpha_eph) for a block of rows
-// plus that block's sum of alpha_eph over rows; the last block to finish sums
-// the block sums (R interleaved groups of blocks, then the groups in order),
-// tabulates psi(sum_i alpha_eph(i,k)) and, when the sweep tracked it, the
-// relative change of S.
-template <typename T, int W>
-__device__ __forceinline__ void finalize_block(const FinInst<T>& p, int blk, int plus_appr,
-                                               int minus_appr) {
-    const long long z = p.z;
-    const int tid = threadIdx.x;
-    if (blk < p.nbB) {
-        const long long idx = (long long)blk * kFinThreads + tid;
-        if (idx < p.y * z) {
-            const long long k = idx % z;
-            const double s = sum_strided<false, W>(p.part_pjk + idx, p.y * z, p.n_rr);
-            if (p.red)
-                p.red[idx] = s;
-            else
-                p.psiB[idx] = T(psi_mode_f64(s + p.beta[k], plus_appr != 0));
-        }
-        return;
-    }
-    __shared__ double acc[2 * kFinThreads];
-    __shared__ unsigned last;
-    const int b = blk - p.nbB;
-    const long long i0 = (long long)b * p.rows_per_ablk;
-    const long long i1 = min(p.x, i0 + p.rows_per_ablk);
-    const int KT = (int)min(z, (long long)kFinThreads);
-    const int R = kFinThreads / KT;
-    const int sub = tid / KT;
-    // R > 1 (z < 256): R row groups of KT threads, combined through acc
-    // (R * z <= 2 * kFinThreads entries); R == 1: a thread's sum over the
-    // block's rows is the block's partial itself (any z)
-    if (sub < R) {
-        for (long long k = tid % KT; k < z; k += KT) {
-            double a = 0.0;
-            for (long long i = i0 + sub; i < i1; i += R) {
-                const double s = sum_strided<false, W>(p.part_ipk + i * z + k, p.x * z, p.n_bands);
-                const double ae = s + p.alpha[i];
-                p.psiA[i * z + k] = T(psi_mode_f64(ae, minus_appr != 0));
-                a += ae;
-            }
-            if (R == 1)
-                p.asum_part[(long long)b * z + k] = a;
-            else
-                acc[sub * z + k] = a;
-        }
-    }
-    if (R > 1) {
-        __syncthreads();
-        for (long long k = tid; k < z; k += kFinThreads) {
-            double a = 0.0;
-            for (int r = 0; r < R; ++r) a += acc[r * z + k];
-            p.asum_part[(long long)b * z + k] = a;
-        }
-    }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) last = (atomicAdd(p.counter, 1u) == (unsigned)(p.n_ablk - 1)) ? 1u : 0u;
-    __syncthreads();
-    if (last) {
-        __threadfence();
-        // group r < R sums blocks r, r + R, r + 2R, ... of column k
-        if (R == 1) {
-            for (long long k = tid; k < z; k += kFinThreads) {
-                const double a = sum_strided<true, W>(p.asum_part + k, z, p.n_ablk);
-                if (p.red)
-                    p.red[p.y * z + k] = a;
-                else
-                    p.psiAS[k] = T(psi_mode_f64(a, minus_appr != 0));
-            }
-        } else {
-            if (sub < R) {
-                for (long long k = tid % KT; k < z; k += KT) {
-                    const int nb = (p.n_ablk - sub + R - 1) / R;
-                    acc[sub * z + k] = sum_strided<true, W>(p.asum_part + (long long)sub * z + k,
-                                                            (long long)R * z, nb);
-                }
-            }
-            __syncthreads();
-            for (long long k = tid; k < z; k += kFinThreads) {
-                double a = 0.0;
-                for (int r = 0; r < R; ++r) a += acc[r * z + k];
-                if (p.red)
-                    p.red[p.y * z + k] = a;
-                else
-                    p.psiAS[k] = T(psi_mode_f64(a, minus_appr != 0));
-            }
-        }
-        if (p.delta_part && tid < 32) {
-            // lanes take tiles t = lane, lane + 32, ...; then a fixed-order tree
-            double d = 0.0, n = 0.0;
-            for (int t = tid; t < p.n_tiles; t += 32) {
-                d += __ldcg(&p.delta_part[2 * t]);
-                n += __ldcg(&p.delta_part[2 * t + 1]);
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                d += __shfl_xor_sync(0xffffffffu, d, o);
-                n += __shfl_xor_sync(0xffffffffu, n, o);
-            }
-            if (tid == 0) *p.rel_change = n > 0.0 ? d / n : (d > 0.0 ? 1.0 : 0.0);
-        }
-        if (tid == 0) *p.counter = 0u;
-    }
-}
 
 template <typename T>
 __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const FinParams<T> p) {
     grid_dep_wait();  // the sweep's partials
     grid_dep_launch();
-    finalize_block<T, 16>(p.f, int(blockIdx.x), p.plus_appr, p.minus_appr);
+    __shared__ double acc[kFinAccDoubles];
+    finalize_block<T, 16>(p.f, int(blockIdx.x), p.plus_appr, p.minus_appr, acc);
 }
 
 // Row-sharded solves: the digamma tables of the shared sums once every shard's
@@ -177,6 +48,28 @@ __global__ void __launch_bounds__(kFinThreads)
     const long long idx = (long long)blockIdx.x * kFinThreads + threadIdx.x;
     if (idx < y * z) psiB[idx] = T(psi_mode_f64(red[idx] + beta[idx % z], plus_appr != 0));
     if (idx < z) psiAS[idx] = T(psi_mode_f64(red[y * z + idx], minus_appr != 0));
+}
+
+void* pick_persist_f32_v4(int lpf, int mch, bool mr);
+void* pick_persist_f32_v1(int lpf, int mch, bool mr);
+void* pick_persist_f64_v2_appr(int lpf, int mch, bool mr);
+void* pick_persist_f64_v2_exact(int lpf, int mch, bool mr);
+void* pick_persist_f64_v1_appr(int lpf, int mch, bool mr);
+void* pick_persist_f64_v1_exact(int lpf, int mch, bool mr);
+
+void* pick_persist_fn(int dtype, int vec, int lpf, int mch, bool multirow, bool appr) {
+    if (dtype == BLDM_F32) {
+        if (vec == 4) return pick_persist_f32_v4(lpf, mch, multirow);
+        if (vec == 1) return pick_persist_f32_v1(lpf, mch, multirow);
+        return nullptr;
+    }
+    if (vec == 2)
+        return appr ? pick_persist_f64_v2_appr(lpf, mch, multirow)
+                    : pick_persist_f64_v2_exact(lpf, mch, multirow);
+    if (vec == 1)
+        return appr ? pick_persist_f64_v1_appr(lpf, mch, multirow)
+                    : pick_persist_f64_v1_exact(lpf, mch, multirow);
+    return nullptr;
 }
 
 // Five resident blocks per SM (48 registers, no spills): a batch's finalize is
@@ -192,7 +85,8 @@ __global__ void __launch_bounds__(kFinThreads, 5) finalize_batch_kernel(const Ba
         else hi = mid - 1;
     }
     const FinInst<T> f = p.insts[lo];
-    finalize_block<T, 8>(f, b - p.block_off[lo], p.plus_appr, p.minus_appr);
+    __shared__ double acc[kFinAccDoubles];
+    finalize_block<T, 8>(f, b - p.block_off[lo], p.plus_appr, p.minus_appr, acc);
 }
 
 void* finalize_batch_fn(int dtype) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "bldm_device.cuh"
+#include "bldm_finalize.cuh"
 #include "bldm_kernels.h"
 
 namespace bldm {
@@ -21,6 +22,11 @@ template <typename T, int VEC> struct VecIO {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) v[e] = __ldg(p + e);
     }
+    // from L2, bypassing L1
+    __device__ __forceinline__ static void ldcg(const T* p, T (&v)[VEC]) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) v[e] = __ldcg(p + e);
+    }
 };
 template <> struct VecIO<double, 2> {
     __device__ __forceinline__ static void load(const double* p, double (&v)[2]) {
@@ -33,6 +39,11 @@ template <> struct VecIO<double, 2> {
     }
     __device__ __forceinline__ static void ldg(const double* p, double (&v)[2]) {
         const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+        v[0] = t.x;
+        v[1] = t.y;
+    }
+    __device__ __forceinline__ static void ldcg(const double* p, double (&v)[2]) {
+        const double2 t = __ldcg(reinterpret_cast<const double2*>(p));
         v[0] = t.x;
         v[1] = t.y;
     }
@@ -55,6 +66,13 @@ template <> struct VecIO<float, 4> {
         v[2] = t.z;
         v[3] = t.w;
     }
+    __device__ __forceinline__ static void ldcg(const float* p, float (&v)[4]) {
+        const float4 t = __ldcg(reinterpret_cast<const float4*>(p));
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    }
 };
 
 __device__ __forceinline__ uintptr_t align_down16(uintptr_t a) { return a & ~uintptr_t(15); }
@@ -65,10 +83,14 @@ __device__ __forceinline__ uintptr_t align_up16(uintptr_t a) {
 // The sweep over one tile (band, row range) of one instance.  Lane layout:
 // lane = g*LPF + q handles fiber slot g of its warp and elements
 // k = (m*LPF + q)*VEC + v; warp w works on row slot w / wpr and column group
-// w % wpr of the band.
+// w % wpr of the band.  Returns false when a bounded wait gave up (the error
+// word is set).  COHERENT: psi(beta_eph) through coherent loads instead of the
+// read-only cache (a persistent kernel reads tables that other CTAs of the
+// same launch rewrote).  FUSED: the tile finalizes its share of the instance in
+// its epilogue (tile_finalize) instead of leaving it to a finalize launch.
 template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool BATCH, bool MULTIROW,
-          bool COMPACT>
-__device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLaunch& L, int band,
+          bool COMPACT, bool COHERENT = false, bool FUSED = false>
+__device__ __forceinline__ bool sweep_tile(const SweepInst<T>& in, const SweepLaunch& L, int band,
                                            int rr, int tile, unsigned char* smem) {
     constexpr int NW = kSweepWarps;
     constexpr int FPW = 32 / LPF;
@@ -125,7 +147,8 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
         nzr[1] = cb[r0 + nrows];
     }
     if (UPDATE)
-        for (long long k = tid; k < z; k += kSweepThreads) sAS[k] = in.psiAS[k];
+        for (long long k = tid; k < z; k += kSweepThreads)
+            sAS[k] = COHERENT ? __ldcg(in.psiAS + k) : in.psiAS[k];
     __syncthreads();
     // entries of the row sequence: the tile's rows, or its listed rows
     const int nlist = compact ? nzr[1] - nzr[0] : nrows;
@@ -217,7 +240,7 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                 for (int u = t; u < issued; ++u)
                     (void)mbar_wait_bounded(&bars[u % L.stages], (uint32_t)((u / L.stages) & 1));
             }
-            return;
+            return false;
         }
         unsigned char* st = stage0 + (size_t)s * L.stage_bytes;
         const bool row_ok = t * RPS + rs < nlist;  // warp-uniform
@@ -401,7 +424,10 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
                         for (int m = 0; m < MCH; ++m) {
                             const long long k0 = (long long)(m * LPF + q) * VEC;
                             if (jl < cw && k0 < z) {
-                                VecIO<T, VEC>::ldg(in.psiB + (c0 + jl) * z + k0, be[m]);
+                                if (COHERENT)
+                                    VecIO<T, VEC>::ldcg(in.psiB + (c0 + jl) * z + k0, be[m]);
+                                else
+                                    VecIO<T, VEC>::ldg(in.psiB + (c0 + jl) * z + k0, be[m]);
                             } else {
 #pragma unroll
                                 for (int v = 0; v < VEC; ++v) be[m][v] = T(0);
@@ -549,6 +575,9 @@ __device__ __forceinline__ void sweep_tile(const SweepInst<T>& in, const SweepLa
             in.delta_part[2 * tile + 1] = b;
         }
     }
+    // the fused finalize in the tile's epilogue (the ring is drained)
+    if (FUSED) tile_finalize<T>(in, L, band, rr, r0, nrows, c0, cw, reinterpret_cast<double*>(stage0));
+    return true;
 }
 
 template <typename T, int VEC, int LPF, int MCH, bool UPDATE, bool APPR, bool MULTIROW,

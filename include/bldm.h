@@ -346,6 +346,29 @@ int bldm_batch_set(bldm_batch* batch, size_t idx, const double* X, const double*
 int bldm_batch_run(bldm_batch* batch, size_t iters, int psi_mode, double eps,
                    int use_graph, void* stream);
 int bldm_batch_check(bldm_batch* batch, void* stream);
+/* Launch form of bldm_batch_run.  persistent = 0 (the default): per iteration,
+ * one sweep launch per lane-shape class (the classes side by side on forked
+ * streams) and one finalize launch for all instances.  persistent = 1: one
+ * persistent launch per class runs every iteration of every instance of the
+ * class from an ordered work queue; each tile finalizes its share of its
+ * instance in its epilogue and an instance moves to its next iteration as soon
+ * as its own previous one is complete (no grid-wide barrier, no per-iteration
+ * launches).  Classes whose fibers need more than two chunks per lane always
+ * use the default form.  The two forms agree to rounding (the sum of alpha_eph
+ * over rows is grouped by row blocks in one and by tile row ranges in the
+ * other); each is deterministic.  On batches of many small instances the
+ * default form is faster: a class of small instances is bound by the latency
+ * of its iterations, and only the side-by-side launches of the default form
+ * overlap the classes.  wait_limit_s bounds each device-side dependency wait
+ * of the persistent form (> 0, <= 60; default 1); when one runs out the run
+ * stops and bldm_batch_check reports BLDM_ERR_TIMEOUT.  stall_test = 1 is for
+ * tests of that failure path only: instance 0's first-iteration tiles then
+ * wait for the completion of that same iteration, so the wait runs out.  No
+ * counterpart in the reference. */
+int bldm_batch_set_launch_mode(bldm_batch* batch, int persistent, double wait_limit_s,
+                               int stall_test);
+/* 1 when bldm_batch_run uses the persistent form for this batch. */
+int bldm_batch_get_launch_mode(const bldm_batch* batch, int* persistent);
 /* Instance idx's S (x*y*z) and the relative change sum|S_n - S_{n-1}| /
  * sum|S_n| of the run's last iteration; either output may be NULL. */
 int bldm_batch_get(bldm_batch* batch, size_t idx, double* S_out, double* rel_change);

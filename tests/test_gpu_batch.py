@@ -257,9 +257,10 @@ def benchmarked_batch(workloads, oracle):
     return shapes, probs, sample, ref
 
 
-def _run_benchmarked(bldm, shapes, probs, ref, dtype):
+def _run_benchmarked(bldm, shapes, probs, ref, dtype, persistent=False):
     import torch
     b = bldm.Batch(shapes, dtype=dtype)
+    b.set_launch_mode(persistent)
     for k, pr in enumerate(probs):
         S0 = ref[k][0] if k in ref else None
         b.set(k, pr["X"], pr["alpha"], pr["beta"], S0, seed=k)
@@ -270,9 +271,11 @@ def _run_benchmarked(bldm, shapes, probs, ref, dtype):
     return b
 
 
-def test_benchmarked_batch_sample_fp64_matches_oracle(bldm, oracle, benchmarked_batch):
+@pytest.mark.parametrize("persistent", [False, True])
+def test_benchmarked_batch_sample_fp64_matches_oracle(bldm, oracle, benchmarked_batch, persistent):
     shapes, probs, sample, ref = benchmarked_batch
-    b = _run_benchmarked(bldm, shapes, probs, ref, bldm.F64)
+    b = _run_benchmarked(bldm, shapes, probs, ref, bldm.F64, persistent)
+    assert b.persistent() == persistent
     cons = b.conservation()
     for k in sample:
         S, _ = b.get(k)
@@ -293,4 +296,105 @@ def test_benchmarked_batch_sample_fp32_log_marginal(bldm, oracle, benchmarked_ba
         lm = oracle.log_marginal_S(S.astype(np.float32), pr["alpha"], pr["beta"], pr["a"],
                                    pr["b"])
         assert abs(lm - ref[k][2]) <= 1e-5 * abs(ref[k][2]), (k, shapes[k], lm, ref[k][2])
+    b.close()
+
+
+def test_persistent_launch_matches_per_iteration_launches(bldm, oracle, workloads):
+    """The persistent form (one launch per class for the whole run, each
+    instance advancing through its own dependencies, the finalize in the tiles'
+    epilogues) against the per-iteration form (a sweep launch per class and a
+    finalize launch per iteration): each bitwise the same with and without the
+    CUDA graph, the two within 1e-12 of each other in FP64 (they group the sum
+    of alpha_eph over rows differently), over two consecutive runs (the second
+    continues from the first's S and digamma tables)."""
+    import torch
+    probs = _problems(workloads, oracle, SHAPES, 61)
+    out = {}
+    for persistent in (True, False):
+        for use_graph in (True, False):
+            b = bldm.Batch(SHAPES, dtype=bldm.F64)
+            b.set_launch_mode(persistent)
+            assert b.persistent() == persistent
+            for k, (X, a, be, S0) in enumerate(probs):
+                b.set(k, X, a, be, S0)
+            stream = torch.cuda.Stream()
+            l0 = b.info()["launches"]
+            b.run(9, use_graph=use_graph, stream=stream)
+            b.run(4, use_graph=use_graph, stream=stream)
+            b.check(stream)
+            n_cls = b.info()["classes"]
+            if persistent:
+                assert b.info()["launches"] - l0 == 2 * n_cls  # one launch per class per run
+            else:
+                assert b.info()["launches"] - l0 == (10 + 5) * (n_cls + 1)
+            out[(persistent, use_graph)] = [b.get(k) for k in range(len(SHAPES))]
+            b.close()
+    for persistent in (True, False):
+        for (S, r), (S0, r0) in zip(out[(persistent, True)], out[(persistent, False)]):
+            np.testing.assert_array_equal(S, S0)
+            assert r == r0
+    for k, ((S, r), (S0, r0)) in enumerate(zip(out[(True, False)], out[(False, False)])):
+        assert rel_err(S, S0) <= 1e-12, (k, rel_err(S, S0))
+        assert abs(r - r0) <= 1e-9 * abs(r0)
+    # and both against the oracle
+    for k, (X, a, be, S0) in enumerate(probs):
+        ref = oracle.bld_mult(X, SHAPES[k][2], a, be, 13, oracle.PSI_APPR, 1e-50, S0=S0)
+        assert rel_err(out[(True, True)][k][0], ref) <= 1e-9
+
+
+def test_persistent_fp64_all_modes(bldm, oracle, workloads):
+    probs = _problems(workloads, oracle, SHAPES[:6], 71)
+    for mode in (0, 1, 2):
+        b = bldm.Batch(SHAPES[:6], dtype=bldm.F64)
+        b.set_launch_mode(True)
+        assert b.persistent()
+        for k, (X, a, be, S0) in enumerate(probs):
+            b.set(k, X, a, be, S0)
+        b.run(8, mode, use_graph=False)
+        b.check()
+        for k, (X, a, be, S0) in enumerate(probs):
+            ref = oracle.bld_mult(X, SHAPES[k][2], a, be, 8, mode, 1e-50, S0=S0)
+            assert rel_err(b.get(k)[0], ref) <= 1e-9, (mode, SHAPES[k])
+        b.close()
+
+
+def test_long_fiber_class_keeps_per_iteration_launches(bldm, oracle, workloads):
+    shapes = [(20, 30, 300), (30, 20, 8)]  # z = 300 in FP32: four chunks per lane
+    probs = _problems(workloads, oracle, shapes, 81)
+    b = bldm.Batch(shapes, dtype=bldm.F32)
+    b.set_launch_mode(True)
+    assert not b.persistent()
+    for k, (X, a, be, S0) in enumerate(probs):
+        b.set(k, X, a, be, S0)
+    b.run(5, use_graph=False)
+    b.check()
+    b.close()
+
+
+def test_persistent_wait_runs_out_and_reports_timeout(bldm, oracle, workloads):
+    """Failure detection without a GPU fault: with the test hook, instance 0's
+    first-iteration tiles wait for the completion of that same iteration;
+    the bounded wait (50 ms) runs out, the launch stops taking work and the
+    host sees BLDM_ERR_TIMEOUT.  The context stays usable: the same batch then
+    runs normally and matches the oracle."""
+    import torch
+    probs = _problems(workloads, oracle, SHAPES[:4], 91)
+    b = bldm.Batch(SHAPES[:4], dtype=bldm.F64)
+    for k, (X, a, be, S0) in enumerate(probs):
+        b.set(k, X, a, be, S0)
+    b.set_launch_mode(True, wait_limit_s=0.05, stall_test=True)
+    stream = torch.cuda.Stream()
+    b.run(3, use_graph=False, stream=stream)
+    with pytest.raises(bldm.BldmError) as ei:
+        b.check(stream)
+    assert ei.value.status == bldm.ERR_TIMEOUT
+    # the error is reported once and cleared; a normal run from fresh S0 works
+    b.set_launch_mode(True, wait_limit_s=1.0, stall_test=False)
+    for k, (X, a, be, S0) in enumerate(probs):
+        b.set(k, X, a, be, S0)
+    b.run(6, use_graph=False, stream=stream)
+    b.check(stream)
+    for k, (X, a, be, S0) in enumerate(probs):
+        ref = oracle.bld_mult(X, SHAPES[k][2], a, be, 6, oracle.PSI_APPR, 1e-50, S0=S0)
+        assert rel_err(b.get(k)[0], ref) <= 1e-9
     b.close()
