@@ -670,8 +670,8 @@ def batch_measure(pkg, torch, args, steps, loop_reps=2, autotune=True):
     tune = None
     if autotune:
         t1 = time.perf_counter()
-        d_ms, t_ms = b.autotune(probe_iters=3, psi_mode=pkg.PSI_APPR, eps=1e-50, stream=stream)
-        tune = {"seconds": time.perf_counter() - t1, "probe_iters": 3,
+        d_ms, t_ms = b.autotune(probe_iters=6, psi_mode=pkg.PSI_APPR, eps=1e-50, stream=stream)
+        tune = {"seconds": time.perf_counter() - t1, "probe_iters": 6,
                 "default_probe_ms": d_ms, "tuned_probe_ms": t_ms,
                 "classes": [{k: c[k] for k in ("vec", "lanes_per_fiber", "chunks", "multirow",
                                                "rows_per_tile", "stages", "tiles", "instances")}
