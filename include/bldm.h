@@ -41,7 +41,8 @@ typedef enum bldm_status {
     BLDM_ERR_CUDA = 4,        /* a CUDA runtime call or launch failed */
     BLDM_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
     BLDM_ERR_NO_DEVICE = 6,   /* no usable CUDA device */
-    BLDM_ERR_UNSUPPORTED = 7, /* shape outside the fused kernels' range (z too large) */
+    BLDM_ERR_UNSUPPORTED = 7, /* batch/server: z beyond the fused kernels' range; a tuning
+                                 the shape cannot take */
     BLDM_ERR_BUSY = 8,        /* serving: no slot or memory for the request now */
     BLDM_ERR_NOT_FOUND = 9,   /* serving: unknown request id */
     BLDM_ERR_TOO_LARGE = 10   /* the shape's scratch exceeds a fixed scratch area */
