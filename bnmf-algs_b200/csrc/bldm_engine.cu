@@ -199,9 +199,12 @@ void Engine::drop_graphs() {
     graphs_.clear();
 }
 
+// SweepInst[n] in instance order; FinInst entries in `fin_order` (the instances
+// of each class together, so that a class's finalize launch takes a slice).
 template <typename T>
 static void fill_tables(const std::vector<EngineInstance*>& insts, std::vector<char>& host,
-                        size_t o_sinst, size_t o_finst, bool skip_zero) {
+                        size_t o_sinst, size_t o_finst, bool skip_zero,
+                        const std::vector<int>& fin_pos) {
     SweepInst<T>* si = reinterpret_cast<SweepInst<T>*>(host.data() + o_sinst);
     FinInst<T>* fi = reinterpret_cast<FinInst<T>*>(host.data() + o_finst);
     for (size_t n = 0; n < insts.size(); ++n) {
@@ -233,7 +236,7 @@ static void fill_tables(const std::vector<EngineInstance*>& insts, std::vector<c
         s.asum_rr = in.asum;
         s.rel_change = in.rel;
         s.done = nullptr;
-        FinInst<T>& f = fi[n];
+        FinInst<T>& f = fi[fin_pos[n]];
         f.red = nullptr;
         f.part_pjk = in.part_pjk;
         f.part_ipk = in.part_ipk;
@@ -392,14 +395,36 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
             counter_bytes_ = cb * 2;
         }
     }
-    // Device tables: SweepInst[n] | FinInst[n] | block_off[n+1] | err | tiles per
-    // class | (persistent) items per class.
+    // Each class's instances, in instance order: the class's finalize launch takes
+    // their FinInst entries (stored together) and block offsets.
+    std::vector<int> fin_pos(n, 0);
+    {
+        int pos = 0;
+        size_t boff_at = 0;
+        for (auto& k : classes_) {
+            k.inst_ids.clear();
+            k.fin_first = pos;
+            k.boff_first = int(boff_at);
+            k.fin_blocks = 0;
+            for (size_t i = 0; i < n; ++i) {
+                const SweepCfg& c = insts[i]->cfg;
+                if (k.vec == c.vec && k.lpf == c.lpf && k.mch == c.mch &&
+                    k.multirow == (c.wpr < kSweepWarps)) {
+                    k.inst_ids.push_back(int(i));
+                    fin_pos[i] = pos++;
+                }
+            }
+            boff_at += k.inst_ids.size() + 1;
+        }
+    }
+    // Device tables: SweepInst[n] | FinInst[n] (by class) | block offsets (per
+    // class, n_c + 1 each) | err | tiles per class | (persistent) items per class.
     const size_t s_sz = dtype_ == BLDM_F64 ? sizeof(SweepInst<double>) : sizeof(SweepInst<float>);
     const size_t f_sz = dtype_ == BLDM_F64 ? sizeof(FinInst<double>) : sizeof(FinInst<float>);
     const size_t o_sinst = 0;
     const size_t o_finst = a256(o_sinst + n * s_sz);
     const size_t o_boff = a256(o_finst + n * f_sz);
-    const size_t o_err = a256(o_boff + (n + 1) * sizeof(int));
+    const size_t o_err = a256(o_boff + (n + classes_.size()) * sizeof(int));
     size_t off = a256(o_err + 64);
     std::vector<size_t> o_tiles(classes_.size()), o_items(classes_.size());
     for (size_t c = 0; c < classes_.size(); ++c) {
@@ -434,17 +459,22 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
     std::vector<char> hv;  // fill_tables works on a vector view of the staging buffer
     hv.resize(o_boff);
     if (dtype_ == BLDM_F64)
-        fill_tables<double>(insts, hv, o_sinst, o_finst, skip_zero_);
+        fill_tables<double>(insts, hv, o_sinst, o_finst, skip_zero_, fin_pos);
     else
-        fill_tables<float>(insts, hv, o_sinst, o_finst, skip_zero_);
+        fill_tables<float>(insts, hv, o_sinst, o_finst, skip_zero_, fin_pos);
     std::memcpy(host, hv.data(), o_boff);
     int* boff = reinterpret_cast<int*>(host + o_boff);
-    fin_blocks_ = 0;
-    for (size_t i = 0; i < n; ++i) {
-        boff[i] = fin_blocks_;
-        fin_blocks_ += insts[i]->nbB + insts[i]->cfg.n_ablk;
+    for (auto& k : classes_) {
+        int* kb = boff + k.boff_first;
+        int blocks = 0;
+        for (size_t j = 0; j < k.inst_ids.size(); ++j) {
+            kb[j] = blocks;
+            const EngineInstance& in = *insts[size_t(k.inst_ids[j])];
+            blocks += in.nbB + in.cfg.n_ablk;
+        }
+        kb[k.inst_ids.size()] = blocks;
+        k.fin_blocks = blocks;
     }
-    boff[n] = fin_blocks_;
     char* base = static_cast<char*>(d_tables_);
     for (size_t c = 0; c < classes_.size(); ++c) {
         std::memcpy(host + o_tiles[c], classes_[c].tiles.data(),
@@ -482,37 +512,23 @@ static void launch_class_kernel(void* fn, unsigned grid, size_t smem, cudaStream
     reinterpret_cast<void (*)(const BatchSweepParams<T>)>(fn)<<<grid, kSweepThreads, smem, s>>>(p);
 }
 
-// The sweeps of one round of every instance: a launch per class, the classes
-// side by side on forked streams.
-int Engine::launch_sweeps(bool update, int psi_mode, bool track, double eps, cudaStream_t st,
-                          bool clean) {
+// One sweep launch of class k on stream s.
+int Engine::launch_class_sweep(ShapeClass& k, cudaStream_t s, bool update, int psi_mode,
+                               bool track, double eps, bool clean) {
     const int plus_appr = psi_mode != BLDM_PSI_EXACT;
     const int minus_appr = psi_mode == BLDM_PSI_APPR;
-    const bool fork = classes_.size() > 1;
-    if (fork) ENG_CU(cudaEventRecord(fork_, st));
-    for (auto& k : classes_) {
-        if (k.tiles.empty()) continue;
-        cudaStream_t s = fork ? k.stream : st;
-        if (fork) ENG_CU(cudaStreamWaitEvent(s, fork_, 0));
-        const int mode = !update ? SWEEP_SUMS : (clean ? SWEEP_COMPACT : SWEEP_UPDATE);
-        void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, mode, plus_appr != 0, true,
-                                 k.multirow);
-        if (dtype_ == BLDM_F64)
-            launch_class_kernel<double>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_,
-                                        k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track,
-                                        plus_appr, minus_appr);
-        else
-            launch_class_kernel<float>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_,
-                                       k.d_tiles, k.stages, k.stage_bytes, eps, d_err_, track,
-                                       plus_appr, minus_appr);
-        ENG_CU(cudaGetLastError());
-        launches_ += 1;
-        if (fork) ENG_CU(cudaEventRecord(k.done, s));
-    }
-    if (fork)
-        for (auto& k : classes_)
-            if (!k.tiles.empty()) ENG_CU(cudaStreamWaitEvent(st, k.done, 0));
-    return BLDM_OK;
+    const int mode = !update ? SWEEP_SUMS : (clean ? SWEEP_COMPACT : SWEEP_UPDATE);
+    void* fn = pick_sweep_fn(dtype_, k.vec, k.lpf, k.mch, mode, plus_appr != 0, true, k.multirow);
+    if (dtype_ == BLDM_F64)
+        launch_class_kernel<double>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_, k.d_tiles,
+                                    k.stages, k.stage_bytes, eps, d_err_, track, plus_appr,
+                                    minus_appr);
+    else
+        launch_class_kernel<float>(fn, unsigned(k.tiles.size()), k.smem, s, d_sinst_, k.d_tiles,
+                                   k.stages, k.stage_bytes, eps, d_err_, track, plus_appr,
+                                   minus_appr);
+    launches_ += 1;
+    return cuda_status(cudaGetLastError());
 }
 
 template <typename T>
@@ -528,26 +544,59 @@ static void launch_fin_kernel(unsigned grid, cudaStream_t s, const void* d_finst
     reinterpret_cast<void (*)(const BatchFinParams<T>)>(fn)<<<grid, kFinThreads, 0, s>>>(p);
 }
 
-// The finalize of every instance in one launch (block_off maps blocks to instances).
-int Engine::launch_finalize(int psi_mode, cudaStream_t st) {
+// The finalize of class k's instances on stream s (block_off maps blocks to them).
+int Engine::launch_class_finalize(ShapeClass& k, cudaStream_t s, int psi_mode) {
     const int plus_appr = psi_mode != BLDM_PSI_EXACT;
     const int minus_appr = psi_mode == BLDM_PSI_APPR;
+    const int* boff = d_block_off_ + k.boff_first;
+    const int nk = int(k.inst_ids.size());
     if (dtype_ == BLDM_F64)
-        launch_fin_kernel<double>(unsigned(fin_blocks_), st, d_finst_, d_block_off_,
-                                  int(insts_.size()), plus_appr, minus_appr);
+        launch_fin_kernel<double>(unsigned(k.fin_blocks), s,
+                                  static_cast<const FinInst<double>*>(d_finst_) + k.fin_first,
+                                  boff, nk, plus_appr, minus_appr);
     else
-        launch_fin_kernel<float>(unsigned(fin_blocks_), st, d_finst_, d_block_off_,
-                                 int(insts_.size()), plus_appr, minus_appr);
+        launch_fin_kernel<float>(unsigned(k.fin_blocks), s,
+                                 static_cast<const FinInst<float>*>(d_finst_) + k.fin_first, boff,
+                                 nk, plus_appr, minus_appr);
     launches_ += 1;
     return cuda_status(cudaGetLastError());
+}
+
+// Each class's rounds on its own forked stream: an instance's round needs only
+// its own class's previous finalize, so the classes never wait for each other
+// until the run's join (a class of small, latency-bound instances overlaps the
+// others instead of adding to every round).
+int Engine::launch_rounds(size_t iters, int psi_mode, double eps, cudaStream_t st, bool prime,
+                          bool clean_first) {
+    const bool fork = classes_.size() > 1;
+    if (fork) ENG_CU(cudaEventRecord(fork_, st));
+    for (auto& k : classes_) {
+        if (k.tiles.empty()) continue;
+        cudaStream_t s = fork ? k.stream : st;
+        if (fork) ENG_CU(cudaStreamWaitEvent(s, fork_, 0));
+        int rc = BLDM_OK;
+        if (prime) {
+            rc = launch_class_sweep(k, s, false, psi_mode, false, eps, false);
+            if (!rc) rc = launch_class_finalize(k, s, psi_mode);
+        }
+        for (size_t it = 0; it < iters && !rc; ++it) {
+            const bool clean = skip_zero_ && (clean_first || it > 0);
+            rc = launch_class_sweep(k, s, true, psi_mode, it + 1 == iters, eps, clean);
+            if (!rc) rc = launch_class_finalize(k, s, psi_mode);
+        }
+        if (rc) return rc;
+        if (fork) ENG_CU(cudaEventRecord(k.done, s));
+    }
+    if (fork)
+        for (auto& k : classes_)
+            if (!k.tiles.empty()) ENG_CU(cudaStreamWaitEvent(st, k.done, 0));
+    return BLDM_OK;
 }
 
 int Engine::prime(int psi_mode, cudaStream_t st) {
     if (psi_mode < BLDM_PSI_EXACT || psi_mode > BLDM_PSI_LEGACY_CUDA) return BLDM_ERR_BAD_ARG;
     if (insts_.empty()) return BLDM_OK;
-    const int rc = launch_sweeps(false, psi_mode, false, 0.0, st, false);
-    if (rc) return rc;
-    return launch_finalize(psi_mode, st);
+    return launch_rounds(0, psi_mode, 0.0, st, true, false);
 }
 
 template <typename T>
@@ -617,21 +666,7 @@ int Engine::launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t
                             bool prime, bool clean_first) {
     if (persistent_active())
         return launch_persistent(iters, psi_mode, eps, st, prime, clean_first);
-    int rc = BLDM_OK;
-    if (prime) {
-        rc = launch_sweeps(false, psi_mode, false, eps, st, false);
-        if (rc) return rc;
-        rc = launch_finalize(psi_mode, st);
-        if (rc) return rc;
-    }
-    for (size_t it = 0; it < iters; ++it) {
-        const bool clean = skip_zero_ && (clean_first || it > 0);
-        rc = launch_sweeps(true, psi_mode, it + 1 == iters, eps, st, clean);
-        if (rc) return rc;
-        rc = launch_finalize(psi_mode, st);
-        if (rc) return rc;
-    }
-    return BLDM_OK;
+    return launch_rounds(iters, psi_mode, eps, st, prime, clean_first);
 }
 
 int Engine::run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStream_t st,
@@ -663,8 +698,10 @@ int Engine::run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStre
         it = graphs_.emplace(key, exec).first;
     }
     ENG_CU(cudaGraphLaunch(it->second, st));
-    launches_ += persistent_active() ? classes_.size()
-                                     : (iters + (prime ? 1 : 0)) * (classes_.size() + 1);
+    size_t active_classes = 0;
+    for (const auto& k : classes_) active_classes += k.tiles.empty() ? 0 : 1;
+    launches_ += persistent_active() ? active_classes
+                                     : (iters + (prime ? 1 : 0)) * 2 * active_classes;
     return BLDM_OK;
 }
 

@@ -2,11 +2,11 @@
 // independent BLD instances of different shapes at once.  Used by the batched
 // solver (bldm_batch_*) and the serving loop (bldm_server_*).
 //
-// An iteration of every instance is one sweep launch per lane-shape class
-// (instances whose z maps to the same kernel), the classes running
-// concurrently on forked streams, then one finalize launch for all instances;
-// or, persistent, one launch per class for a whole run whose tiles finalize
-// their instances in their epilogues.
+// An iteration of the instances of one lane-shape class (instances whose z
+// maps to the same kernel) is one sweep launch and one finalize launch; each
+// class runs its iterations on its own forked stream, the classes joining at
+// the end of a run.  Or, persistent, one launch per class for a whole run
+// whose tiles finalize their instances in their epilogues.
 // Tiles (band x row range) of every instance of a class form the class grid;
 // the tiling of an instance depends only on its own shape, so its results do
 // not depend on which other instances share the launches.
@@ -153,6 +153,11 @@ class Engine {
         cudaStream_t stream = nullptr;
         cudaEvent_t done = nullptr;
         // persistent launch of the class
+        // the class's instances and its slice of the finalize tables
+        std::vector<int> inst_ids;
+        int fin_first = 0;   // first FinInst of the class
+        int boff_first = 0;  // first block offset of the class
+        int fin_blocks = 0;  // finalize blocks of the class
         void* pfn[2] = {nullptr, nullptr};  // by digamma of grad_plus: exact, psi_appr
         std::vector<PItem> items;  // one round: the tiles, largest first
         PItem* d_items = nullptr;
@@ -162,9 +167,11 @@ class Engine {
                           bool clean_first);
     int launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t st, bool prime,
                         bool clean_first);
-    int launch_sweeps(bool update, int psi_mode, bool track, double eps, cudaStream_t st,
-                      bool clean);
-    int launch_finalize(int psi_mode, cudaStream_t st);
+    int launch_class_sweep(ShapeClass& k, cudaStream_t s, bool update, int psi_mode, bool track,
+                           double eps, bool clean);
+    int launch_class_finalize(ShapeClass& k, cudaStream_t s, int psi_mode);
+    int launch_rounds(size_t iters, int psi_mode, double eps, cudaStream_t st, bool prime,
+                      bool clean_first);
     void free_tables();
     void drop_graphs();
 
@@ -183,7 +190,6 @@ class Engine {
     void* d_sinst_ = nullptr;
     void* d_finst_ = nullptr;
     int* d_block_off_ = nullptr;
-    int fin_blocks_ = 0;
     int* d_err_ = nullptr;
     cudaEvent_t fork_ = nullptr;
     uint64_t launches_ = 0;

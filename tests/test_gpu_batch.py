@@ -326,7 +326,8 @@ def test_persistent_launch_matches_per_iteration_launches(bldm, oracle, workload
             if persistent:
                 assert b.info()["launches"] - l0 == 2 * n_cls  # one launch per class per run
             else:
-                assert b.info()["launches"] - l0 == (10 + 5) * (n_cls + 1)
+                # a sweep and a finalize launch per class and iteration (prime included)
+                assert b.info()["launches"] - l0 == (10 + 5) * 2 * n_cls
             out[(persistent, use_graph)] = [b.get(k) for k in range(len(SHAPES))]
             b.close()
     for persistent in (True, False):
