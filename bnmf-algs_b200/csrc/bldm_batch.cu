@@ -296,7 +296,7 @@ int bldm_batch_autotune(bldm_batch* b, size_t probe_iters, int psi_mode, double 
         int r = rebuild(b, st);
         if (r) return r;
         double best = 1e300;
-        for (int rep = 0; rep < 2; ++rep) {
+        for (int rep = 0; rep < 3; ++rep) {
             r = copy_S(start, false);
             if (r) return r;
             cudaEventRecord(e0, st);
@@ -345,7 +345,7 @@ int bldm_batch_autotune(bldm_batch* b, size_t probe_iters, int psi_mode, double 
                 rc = r;
                 break;
             }
-            if (ms < 0.98 * best) {
+            if (ms < 0.97 * best) {
                 best = ms;
                 cur.rows_per_tile = R;
             }
@@ -361,7 +361,7 @@ int bldm_batch_autotune(bldm_batch* b, size_t probe_iters, int psi_mode, double 
                 rc = r;
                 break;
             }
-            if (ms < 0.98 * best) {
+            if (ms < 0.97 * best) {
                 best = ms;
                 cur.stages = S;
             }

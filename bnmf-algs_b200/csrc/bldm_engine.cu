@@ -424,7 +424,9 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
     const size_t o_sinst = 0;
     const size_t o_finst = a256(o_sinst + n * s_sz);
     const size_t o_boff = a256(o_finst + n * f_sz);
-    const size_t o_err = a256(o_boff + (n + classes_.size()) * sizeof(int));
+    // per-class offsets (n_c + 1 each), then the offsets of all instances (n + 1)
+    const size_t n_boff = (n + classes_.size()) + (n + 1);
+    const size_t o_err = a256(o_boff + n_boff * sizeof(int));
     size_t off = a256(o_err + 64);
     std::vector<size_t> o_tiles(classes_.size()), o_items(classes_.size());
     for (size_t c = 0; c < classes_.size(); ++c) {
@@ -474,6 +476,19 @@ int Engine::build(const std::vector<EngineInstance*>& insts, cudaStream_t st) {
         }
         kb[k.inst_ids.size()] = blocks;
         k.fin_blocks = blocks;
+    }
+    {
+        // all instances in the FinInst order (the classes one after the other)
+        int* ab = boff + n + classes_.size();
+        int blocks = 0, j = 0;
+        for (auto& k : classes_)
+            for (int i : k.inst_ids) {
+                ab[j++] = blocks;
+                blocks += insts[size_t(i)]->nbB + insts[size_t(i)]->cfg.n_ablk;
+            }
+        ab[n] = blocks;
+        fin_blocks_all_ = blocks;
+        boff_all_first_ = int(n + classes_.size());
     }
     char* base = static_cast<char*>(d_tables_);
     for (size_t c = 0; c < classes_.size(); ++c) {
@@ -593,10 +608,57 @@ int Engine::launch_rounds(size_t iters, int psi_mode, double eps, cudaStream_t s
     return BLDM_OK;
 }
 
+// One finalize launch for every instance (the joined form).
+int Engine::launch_finalize_all(cudaStream_t st, int psi_mode) {
+    const int plus_appr = psi_mode != BLDM_PSI_EXACT;
+    const int minus_appr = psi_mode == BLDM_PSI_APPR;
+    const int* boff = d_block_off_ + boff_all_first_;
+    const int n = int(insts_.size());
+    if (dtype_ == BLDM_F64)
+        launch_fin_kernel<double>(unsigned(fin_blocks_all_), st,
+                                  static_cast<const FinInst<double>*>(d_finst_), boff, n,
+                                  plus_appr, minus_appr);
+    else
+        launch_fin_kernel<float>(unsigned(fin_blocks_all_), st,
+                                 static_cast<const FinInst<float>*>(d_finst_), boff, n,
+                                 plus_appr, minus_appr);
+    launches_ += 1;
+    return cuda_status(cudaGetLastError());
+}
+
+// The joined form: per iteration, the classes' sweeps side by side on forked
+// streams, a join, and one finalize launch for every instance (fewer launches
+// than the per-class form: for callers that launch rounds directly).
+int Engine::launch_rounds_joined(size_t iters, int psi_mode, double eps, cudaStream_t st,
+                                 bool prime, bool clean_first) {
+    const bool fork = classes_.size() > 1;
+    auto sweeps = [&](bool update, bool track, bool clean) -> int {
+        if (fork) ENG_CU(cudaEventRecord(fork_, st));
+        for (auto& k : classes_) {
+            if (k.tiles.empty()) continue;
+            cudaStream_t s = fork ? k.stream : st;
+            if (fork) ENG_CU(cudaStreamWaitEvent(s, fork_, 0));
+            const int rc = launch_class_sweep(k, s, update, psi_mode, track, eps, clean);
+            if (rc) return rc;
+            if (fork) ENG_CU(cudaEventRecord(k.done, s));
+        }
+        if (fork)
+            for (auto& k : classes_)
+                if (!k.tiles.empty()) ENG_CU(cudaStreamWaitEvent(st, k.done, 0));
+        return launch_finalize_all(st, psi_mode);
+    };
+    int rc = BLDM_OK;
+    if (prime) rc = sweeps(false, false, false);
+    for (size_t it = 0; it < iters && !rc; ++it)
+        rc = sweeps(true, it + 1 == iters, skip_zero_ && (clean_first || it > 0));
+    return rc;
+}
+
 int Engine::prime(int psi_mode, cudaStream_t st) {
     if (psi_mode < BLDM_PSI_EXACT || psi_mode > BLDM_PSI_LEGACY_CUDA) return BLDM_ERR_BAD_ARG;
     if (insts_.empty()) return BLDM_OK;
-    return launch_rounds(0, psi_mode, 0.0, st, true, false);
+    return per_class_rounds_ ? launch_rounds(0, psi_mode, 0.0, st, true, false)
+                             : launch_rounds_joined(0, psi_mode, 0.0, st, true, false);
 }
 
 template <typename T>
@@ -666,6 +728,8 @@ int Engine::launch_sequence(size_t iters, int psi_mode, double eps, cudaStream_t
                             bool prime, bool clean_first) {
     if (persistent_active())
         return launch_persistent(iters, psi_mode, eps, st, prime, clean_first);
+    if (!per_class_rounds_)
+        return launch_rounds_joined(iters, psi_mode, eps, st, prime, clean_first);
     return launch_rounds(iters, psi_mode, eps, st, prime, clean_first);
 }
 
@@ -700,8 +764,9 @@ int Engine::run(size_t iters, int psi_mode, double eps, bool use_graph, cudaStre
     ENG_CU(cudaGraphLaunch(it->second, st));
     size_t active_classes = 0;
     for (const auto& k : classes_) active_classes += k.tiles.empty() ? 0 : 1;
-    launches_ += persistent_active() ? active_classes
-                                     : (iters + (prime ? 1 : 0)) * 2 * active_classes;
+    launches_ += persistent_active()   ? active_classes
+                 : per_class_rounds_ ? (iters + (prime ? 1 : 0)) * 2 * active_classes
+                                     : (iters + (prime ? 1 : 0)) * (active_classes + 1);
     return BLDM_OK;
 }
 

@@ -133,6 +133,15 @@ class Engine {
         drop_graphs();
     }
     bool persistent_active() const { return persistent_ && persist_ok_; }
+    // Per-iteration launches: every class on its own stream with its own
+    // finalize launch, joining once per run (the default: fewest waits, best in
+    // a captured graph), or, joined, the classes' sweeps side by side and one
+    // finalize launch for all instances per iteration (fewer launches, for
+    // callers that launch rounds directly).  Both give bitwise the same results.
+    void set_per_class_rounds(bool on) {
+        per_class_rounds_ = on;
+        drop_graphs();
+    }
 
     int dtype() const { return dtype_; }
     size_t es() const { return es_; }
@@ -172,6 +181,9 @@ class Engine {
     int launch_class_finalize(ShapeClass& k, cudaStream_t s, int psi_mode);
     int launch_rounds(size_t iters, int psi_mode, double eps, cudaStream_t st, bool prime,
                       bool clean_first);
+    int launch_finalize_all(cudaStream_t st, int psi_mode);
+    int launch_rounds_joined(size_t iters, int psi_mode, double eps, cudaStream_t st,
+                             bool prime, bool clean_first);
     void free_tables();
     void drop_graphs();
 
@@ -197,6 +209,9 @@ class Engine {
     // persistent launches: the counters cleared before every run (rounds done
     // per instance [n] | queue control per class)
     bool persistent_ = false;
+    bool per_class_rounds_ = true;
+    int fin_blocks_all_ = 0;
+    int boff_all_first_ = 0;
     bool persist_ok_ = false;
     bool stall_test_ = false;
     unsigned long long wait_ns_ = 1000000000ull;

@@ -449,6 +449,10 @@ int bldm_server_create(bldm_server** out, const bldm_server_config* cfg) {
         Lane& L = s->lanes[l];
         L.eng.reset(new Engine(cfg->dtype, cfg->rows_per_tile));
         L.primer.reset(new Engine(cfg->dtype, cfg->rows_per_tile));
+        // the worker launches each round directly (its set of requests changes
+        // from round to round): the joined form's fewer launches
+        L.eng->set_per_class_rounds(false);
+        L.primer->set_per_class_rounds(false);
         L.h_rel.assign(cfg->max_active, 1.0);
         e = cudaStreamCreateWithPriority(&L.stream, cudaStreamNonBlocking,
                                          l == 0 ? prio_high : prio_low);

@@ -401,10 +401,10 @@ int bldm_batch_class_info(const bldm_batch* batch, size_t idx, bldm_batch_class*
 int bldm_batch_set_class(bldm_batch* batch, const bldm_batch_class* c);
 /* Autotuner: for each class, largest first, tries tile heights
  * {32, 64, 128, 256, 512} and stage depths {2, 3, 4, 6, 8}, timing
- * probe_iters iterations of the whole batch (CUDA events, best of two) in the
- * steady state of a run (from the S after one update, skipping zero rows from
- * the first probe iteration on), and keeps a change when the batch gets at
- * least 2% faster.  S is saved on the device and restored afterwards, so the
+ * probe_iters iterations of the whole batch (CUDA events, best of three) in
+ * the steady state of a run (from the S after one update, skipping zero rows
+ * from the first probe iteration on), and keeps a change when the batch gets
+ * at least 3% faster.  S is saved on the device and restored afterwards, so the
  * call does not change the solution.  Call after bldm_batch_set of every
  * instance.
  * default_ms / tuned_ms (nullable): probe time before and after. */
