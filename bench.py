@@ -78,11 +78,13 @@ def profile_value(name, key="traffic_bytes_per_launch"):
 
 
 def kernel_source_sha():
-    """Digest of the sweep kernel sources, to compare with a profile's
-    kernel_source_sha line: equal means the capture is of this build's kernel."""
+    """Digest of the files that hold the update sweep's code (the tile function,
+    the digamma and bulk-copy helpers, the finalize it includes), to compare
+    with a profile's kernel_source_sha line: equal means the capture is of this
+    build's kernel."""
     import hashlib
     h = hashlib.sha256()
-    for f in ("bldm_sweep_kernels.cuh", "bldm_device.cuh", "bldm_kernels.h"):
+    for f in ("bldm_sweep_kernels.cuh", "bldm_device.cuh", "bldm_finalize.cuh"):
         with open(os.path.join(PKG_DIR, "csrc", f), "rb") as fh:
             h.update(fh.read())
     return h.hexdigest()[:12]
