@@ -199,9 +199,10 @@ int bldm_batch_conservation(bldm_batch* b, double* residuals, void* stream) {
     int blocks = 0;
     for (size_t i = 0; i < n; ++i) {
         const EngineInstance& in = b->inst[i];
-        ci[i] = cons_inst(in.X, in.S, (long long)(in.x * in.y), (long long)in.z, d_out + i);
+        ci[i] = cons_inst(b->dtype, in.X, in.S, (long long)(in.x * in.y), (long long)in.z,
+                          d_out + i);
         boff[i] = blocks;
-        blocks += conservation_blocks((long long)(in.x * in.y), (long long)in.z);
+        blocks += conservation_blocks(b->dtype, in.S, (long long)(in.x * in.y), (long long)in.z);
     }
     boff[n] = blocks;
     int rc = cuda_status(cudaMemcpyAsync(base, host.data(), bytes, cudaMemcpyHostToDevice, st));

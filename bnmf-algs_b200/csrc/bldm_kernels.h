@@ -209,12 +209,12 @@ struct ConsInst {
     const void* S;
     long long nf, z;
     unsigned long long* out;
-    int lpf, pad;
+    int lpf, pad;  // lanes per fiber; pad: elements per vector load
 };
 int launch_conservation_multi(int dtype, const ConsInst* d_insts, const int* d_block_off,
                               int n_inst, int n_blocks, cudaStream_t st);
-int conservation_blocks(long long nf, long long z);
-ConsInst cons_inst(const void* X, const void* S, long long nf, long long z,
+int conservation_blocks(int dtype, const void* dS, long long nf, long long z);
+ConsInst cons_inst(int dtype, const void* X, const void* S, long long nf, long long z,
                    unsigned long long* out);
 // The residual from the bits launch_conservation left.
 double cons_value(unsigned long long bits);

@@ -359,6 +359,11 @@ def test_conservation_residual_matches_numpy(bldm, oracle, workloads, dtype_name
     dX = dev(X, tt)
     assert plan.conservation(dX, dev(S, tt)) == pytest.approx(want, rel=tol, abs=tol)
     assert plan.conservation(dX, dev(S0, tt)) <= (1e-14 if f64 else 1e-6)
+    # S one element past a 16-byte boundary: scalar loads instead of 16-byte ones
+    buf = torch.empty(S.size + 1, dtype=tt, device="cuda")
+    buf[1:] = dev(S, tt).reshape(-1)
+    assert buf[1:].data_ptr() % 16 != 0
+    assert plan.conservation(dX, buf[1:]) == pytest.approx(want, rel=tol, abs=tol)
     plan.close()
 
 
