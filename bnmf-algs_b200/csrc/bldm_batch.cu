@@ -20,6 +20,7 @@ struct bldm_batch {
     size_t arena_bytes = 0;
     int dtype = BLDM_F64;
     bool clean = false;  // every instance has been updated since its S was set
+    bool reorder = false;  // an X was set since the last build: re-sort the tiles
     void* cons_buf = nullptr;  // conservation: ConsInst[n] | block_off[n+1] | residual bits[n]
     ~bldm_batch() {
         eng.reset();
@@ -49,7 +50,9 @@ int download(const void* src, size_t n, double* dst) {
 // Re-tiles every instance from the engine's class tunings and rebuilds.
 int rebuild(bldm_batch* b, cudaStream_t st) {
     for (auto& in : b->inst) b->eng->retile(in);
-    return b->eng->build(b->ptrs, st);
+    const int rc = b->eng->build(b->ptrs, st);
+    if (rc == BLDM_OK) b->reorder = false;
+    return rc;
 }
 
 }  // namespace
@@ -119,6 +122,8 @@ int bldm_batch_set(bldm_batch* b, size_t idx, const double* X, const double* alp
     if (rc) return rc;
     rc = b->eng->set_row_lists(in, nullptr);
     if (rc) return rc;
+    b->eng->set_work(in, X, true);
+    b->reorder = true;
     rc = cuda_status(cudaMemcpy(in.alpha, alpha, in.x * 8, cudaMemcpyHostToDevice));
     if (rc) return rc;
     rc = cuda_status(cudaMemcpy(in.beta, beta, in.z * 8, cudaMemcpyHostToDevice));
@@ -138,6 +143,11 @@ int bldm_batch_set(bldm_batch* b, size_t idx, const double* X, const double* alp
 int bldm_batch_run(bldm_batch* b, size_t iters, int psi_mode, double eps, int use_graph,
                    void* stream) {
     if (!b) return BLDM_ERR_BAD_ARG;
+    if (b->reorder) {
+        // the tiles in the order of the work estimates of the X values set
+        const int rr = rebuild(b, static_cast<cudaStream_t>(stream));
+        if (rr) return rr;
+    }
     const int rc = b->eng->run(iters, psi_mode, eps, use_graph != 0,
                                static_cast<cudaStream_t>(stream), true, b->clean);
     if (rc == BLDM_OK && iters > 0) b->clean = true;

@@ -65,6 +65,10 @@ struct EngineInstance {
     double* rel = nullptr;
     int* nz_rows = nullptr;  // [n_bands][x] rows with X != 0 per band, ascending
     int* nz_cnt = nullptr;   // [n_bands][x + 1] running counts of nz_rows
+    // Host-side work estimate (Engine::set_work; empty: tiles weigh their bytes):
+    // per band, running counts over the rows of the rows whose band segment of X
+    // has a nonzero and of the nonzero passes.  [n_bands][x + 1] each.
+    std::vector<int> work_rows, work_pass;
 };
 
 // Byte sizes of an instance's buffers, in the order of EngineInstance's fields.
@@ -105,6 +109,13 @@ class Engine {
 
     // Row lists of the instance's band segments with X != 0 (after X is set).
     int set_row_lists(EngineInstance& in, cudaStream_t st) const;
+    // Work estimate of the instance's tiles from its X on the host (x * y
+    // elements, FP64 or FP32 by f64), used to order the tiles of the next
+    // builds.  A compact update sweeps only the rows of a band segment with a
+    // nonzero and runs the update arithmetic only for the passes (32 / lpf
+    // adjacent columns) with one, so instances of equal shape can differ in
+    // work many times over.
+    void set_work(EngineInstance& in, const void* X, bool f64) const;
     // (Re)builds the launch tables for the given instances; the pointers must
     // stay valid until the next build.  Clears the per-instance counters on st.
     int build(const std::vector<EngineInstance*>& insts, cudaStream_t st);
