@@ -260,9 +260,12 @@ template <> struct PsiPass<double, false> {
 // at v + 3 >= 4 (and at v >= 4 unshifted) the asymptotic series
 // ln x - 1/(2x) - sum_k B_2k / (2k x^2k), truncated after the x^-10 term,
 // leaves a remainder below 1.3e-9, under FP32 resolution.  One reciprocal of
-// x q serves both 1/x and the shift's division; the logarithm is the hardware
-// base-2 one (relative error about 2^-21, at the resolution of FP32 S).  No
-// per-step selects: the shift is a fixed polynomial evaluation.
+// x q serves both 1/x and the shift's division: the hardware approximation
+// alone (about one ulp; a Newton step would not show beside the logarithm's
+// error, and FP32 S computed with it is as unbiased against FP64 as with the
+// refined reciprocal).  The logarithm is the hardware base-2 one (relative
+// error about 2^-21, at the resolution of FP32 S).  No per-step selects: the
+// shift is a fixed polynomial evaluation.
 template <int NE>
 __device__ __forceinline__ void psi_f32_batch(const float (&x)[NE], float (&out)[NE]) {
 #pragma unroll
@@ -272,7 +275,8 @@ __device__ __forceinline__ void psi_f32_batch(const float (&x)[NE], float (&out)
         const float q = lo ? fmaf(v + 3.0f, v, 2.0f) * v : 1.0f;   // v (v+1) (v+2)
         const float p = lo ? fmaf(fmaf(3.0f, v, 6.0f), v, 2.0f) : 0.0f;
         const float xs = lo ? v + 3.0f : v;
-        const float inv = Rcp<float>::of(xs * q);
+        float inv;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(xs * q));
         const float r = q * inv;              // 1 / xs
         const float shift = lo ? (p * xs) * inv : 0.0f;   // p / q (no 0 * inf at v = inf)
         const float r2 = r * r;

@@ -12,10 +12,12 @@ namespace {
 size_t a256(size_t v) { return (v + 255) & ~size_t(255); }
 
 // Cost of an element of a nonzero pass's update arithmetic relative to an
-// element swept (chosen by timing the z = 64 class of the 512-instance uneven
-// batch, X densities 1% to 89%: weights 0 (bytes), 2 and 6 gave 506, 521 and
-// 469 us per iteration).
-constexpr double kPassWork = 6.0;
+// element swept, chosen by timing the 512-instance uneven batch (FP32, X
+// densities 1% to 89%) and its z = 64 class alone: weights 0 (bytes order), 2,
+// 6, 16, 40 and 120 gave 113.5, 113.3, 112.4, 111.7, 110.7 and 110.9 ms per
+// 150-iteration run of the batch and 506, 521, 469, 444, 415 and 408 us per
+// iteration of the class.
+constexpr double kPassWork = 40.0;
 
 int sms_of_current_device() {
     int dev = 0, n = 0;
