@@ -111,7 +111,8 @@ class Engine {
     int set_row_lists(EngineInstance& in, cudaStream_t st) const;
     // Work estimate of the instance's tiles from its X on the host (x * y
     // elements, FP64 or FP32 by f64), used to order the tiles of the next
-    // builds.  A compact update sweeps only the rows of a band segment with a
+    // builds (the batch sets it; the server, whose rounds hold few instances
+    // and whose admission is on every request's latency path, does not).  A compact update sweeps only the rows of a band segment with a
     // nonzero and runs the update arithmetic only for the passes (32 / lpf
     // adjacent columns) with one, so instances of equal shape can differ in
     // work many times over.

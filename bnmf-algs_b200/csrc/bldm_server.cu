@@ -194,10 +194,6 @@ int bldm_server::admit(Lane& L, Request* r) {
     if (e != cudaSuccess) return cuda_status(e);
     rc = eng->set_row_lists(r->inst, stream);
     if (rc) return rc;
-    if (eng->es() == 8)
-        eng->set_work(r->inst, r->X.data(), true);
-    else
-        eng->set_work(r->inst, r->Xf.data(), false);
     return launch_init_S(eng->dtype(), r->inst.X, r->inst.S, (long long)(r->x * r->y),
                          (long long)r->z, r->seed, stream);
 }
