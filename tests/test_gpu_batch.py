@@ -399,3 +399,57 @@ def test_persistent_wait_runs_out_and_reports_timeout(bldm, oracle, workloads):
         ref = oracle.bld_mult(X, SHAPES[k][2], a, be, 6, oracle.PSI_APPR, 1e-50, S0=S0)
         assert rel_err(b.get(k)[0], ref) <= 1e-9
     b.close()
+
+
+def test_tile_order_follows_x_and_changes_no_result(bldm, oracle, workloads):
+    """The engine orders a class's tiles by the work its X implies (rows with a
+    nonzero, nonzero passes), not by bytes.  Instances of very different
+    densities in forward and reversed order, and a batch re-sorted after one
+    instance's X is set again, give every instance bitwise the same S as a
+    batch set up with the final X from the start."""
+    shapes = [(96, 130, 64), (64, 200, 64), (150, 90, 64), (40, 260, 64), (120, 120, 64)]
+    probs = []
+    for k, (x, y, z) in enumerate(shapes):
+        rng = np.random.default_rng(50 + k)
+        if k % 2 == 0:
+            X = 1.0 + rng.poisson(10.0, (x, y)).astype(float)  # every fiber works
+        else:
+            X = workloads.allocation_model_X(x, y, z, 5.0, 0.05, rng)  # mostly zeros
+        probs.append((X, rng.uniform(1.0, 2.0, x), rng.uniform(1.0, 2.0, z),
+                      oracle.init_S(X, z, 50 + k)))
+
+    def solve(order, iters=12):
+        b = bldm.Batch([shapes[k] for k in order], dtype=bldm.F32)
+        for i, k in enumerate(order):
+            X, a, be, S0 = probs[k]
+            b.set(i, X, a, be, S0)
+        b.run(iters, use_graph=True)
+        b.check()
+        out = {k: b.get(i)[0] for i, k in enumerate(order)}
+        return b, out
+
+    fwd, S_fwd = solve(list(range(len(shapes))))
+    rev, S_rev = solve(list(reversed(range(len(shapes)))))
+    rev.close()
+    for k in range(len(shapes)):
+        np.testing.assert_array_equal(S_fwd[k], S_rev[k])
+    # instance 1 becomes dense: the next run re-sorts the tiles
+    x, y, z = shapes[1]
+    X1 = 1.0 + np.random.default_rng(99).poisson(10.0, (x, y)).astype(float)
+    probs[1] = (X1, probs[1][1], probs[1][2], oracle.init_S(X1, z, 99))
+    for k in range(len(shapes)):
+        X, a, be, S0 = probs[k]
+        fwd.set(k, X, a, be, S0)
+    fwd.run(12, use_graph=True)
+    fwd.check()
+    fresh, S_fresh = solve(list(range(len(shapes))))
+    fresh.close()
+    for k in range(len(shapes)):
+        np.testing.assert_array_equal(fwd.get(k)[0], S_fresh[k])
+    # and the FP32 solve of the dense instance keeps this file's FP32 bound
+    ref = oracle.bld_mult(X1, z, probs[1][1], probs[1][2], 12, oracle.PSI_APPR, 1e-50,
+                          S0=probs[1][3])
+    ref32 = oracle.bld_mult(X1, z, probs[1][1], probs[1][2], 12, oracle.PSI_APPR, 1e-50,
+                            S0=probs[1][3], dtype=np.float32)
+    assert rel_err(S_fresh[1], ref) <= max(1e-5, 10 * rel_err(ref32, ref))
+    fwd.close()
