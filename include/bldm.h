@@ -326,10 +326,12 @@ int bldm_sample_X(const void* d_W, const void* d_H, const void* d_L, size_t x, s
  * its class's launch shape, so its result does not depend on the other
  * instances of the batch; it agrees with bldm_plan_run's to rounding (the
  * partial sums are grouped by tile).  One iteration of every instance is one
- * fused-sweep launch per lane-shape class (instances whose z maps to the same
- * kernel), the classes concurrent on forked streams, and one finalize launch
- * for all instances; with use_graph the whole run is captured once per
- * (iters, psi_mode, eps) into a CUDA graph and replayed.
+ * fused-sweep launch and one finalize launch per lane-shape class (instances
+ * whose z maps to the same kernel), each class running its iterations on its
+ * own forked stream; with use_graph the whole run is captured once per
+ * (iters, psi_mode, eps) into a CUDA graph and replayed.  A class's tiles run
+ * heaviest first by the work their X implies (rows with a nonzero, passes
+ * with a nonzero); the order changes no result.
  * rows_per_tile (0 = 64) is the default tile height (rows of S per CTA tile)
  * of every class; bldm_batch_autotune picks it and the stage-ring depth per
  * class from timed probe runs on the batch's own data.
@@ -339,7 +341,9 @@ typedef struct bldm_batch bldm_batch;
 int bldm_batch_create(bldm_batch** batch, int dtype, size_t n, const size_t* xs,
                       const size_t* ys, const size_t* zs, int rows_per_tile);
 int bldm_batch_destroy(bldm_batch* batch);
-/* Instance idx's data; S0 NULL draws the seeded initial S on the device. */
+/* Instance idx's data; S0 NULL draws the seeded initial S on the device.
+ * The next bldm_batch_run first rebuilds the launch tables in the tile order
+ * of the X values set (host work on that call only). */
 int bldm_batch_set(bldm_batch* batch, size_t idx, const double* X, const double* alpha,
                    const double* beta, const double* S0, uint64_t seed);
 /* Runs `iters` iterations of every instance from its current S (asynchronous
